@@ -1,0 +1,347 @@
+"""Benchmark: stability-boundary points per second on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload ("sweep"): one milling setup -- 4 flutes, D 10 mm, helix 30 deg, 10 um runout,
+Ktc 700 / Krc 210 / Kte 20 / Kre 30, 3 modes per axis (fn 600-3000 Hz, k 5e6-5e7 N/m,
+zeta 0.01-0.05, seeded) -- swept over 4096 spindle speeds 3000-30000 rpm; each speed is a
+10-iteration geometric bisection over [0.05, 15] mm whose trials run 60 revolutions with
+40 slices and the reference's steps-per-tooth rule.  A step = the whole 4096-point sweep.
+
+`value`  points/s with the inputs resident on the device: the prepared batch is a
+         captured CUDA graph (mcs_plan_execute), timed with CUDA events on the library's
+         stream, L2 flushed (a 256 MiB write) between timed steps.
+`e2e`    the same through the public blocking call mcs_solve from page-locked host
+         buffers: host preparation, H2D copies, the solve and the D2H of results per step.
+Multi-GPU (torchrun): every rank solves its own seeded 4096-point sweep (weak scaling, no
+collective on the data path); the time is the max over ranks.
+
+--impl reference: the reference's CPU path on the host cores.  The reference is
+JavaScript and no JS runtime exists on these machines, so this arm times the C++ FP64
+restatement of it (oracle/) with one thread per core on a bounded sample of the sweep.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "machinig-sim_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+METRIC = "stability-boundary points/sec on 1 B200: surrogate-guided vs plain GPU vs Node CPU @<=2% depth err"
+UNIT = "points/s"
+FLOP_ENGAGED = 46.0   # FP32 flop per in-cut slice evaluation (force law, cutting.js:181-207)
+FLOP_IDLE = 15.0      # per out-of-cut evaluation of the reference loop (angle, normal, store)
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_oracle_sample(wl, n_points: int, threads: int):
+    """FP64 oracle over the first n_points of a seeded permutation of the workload."""
+    import pyoracle as O
+    from mcs import _abi as A
+
+    perm = np.argsort(np.random.default_rng(7).random(wl.n))[:n_points]
+    setups = [A.Setup.from_buffer_copy(r.tobytes()) for r in wl.setups]
+    modals = [A.Modal.from_buffer_copy(r.tobytes()) for r in wl.modals]
+    pts = wl.points[np.sort(perm)]
+    P = (A.Point * len(pts)).from_buffer_copy(pts.tobytes())
+    t = time.perf_counter()
+    O.solve_batch(setups, modals, P, wl.opts, nthreads=threads)
+    return len(pts), time.perf_counter() - t
+
+
+def cpu_baseline(wl, target_s: float = 15.0) -> dict:
+    cores = cpu_cores()
+    n = min(wl.n, max(16, 2 * cores))
+    npts, dt = run_oracle_sample(wl, n, cores)
+    if dt < target_s / 3 and npts < wl.n:  # too short to be a stable figure: grow once
+        n2 = min(wl.n, int(npts * target_s / max(dt, 1e-3) * 0.5))
+        if n2 > npts:
+            npts, dt = run_oracle_sample(wl, n2, cores)
+    return {"value": npts / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{npts} of the {wl.n} sweep points (seeded), C++ FP64 restatement of "
+                      f"stabtd.js/cutting.js, {cores} threads on {cpu_model()}"}
+
+
+def reference_arm(args) -> int:
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from mcs import workloads as W
+
+    wl = W.sweep()
+    cores = cpu_cores()
+    n = min(wl.n, max(8, cores))
+    for _ in range(args.warmup):
+        run_oracle_sample(wl, n, cores)
+    tot_p, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        p, t = run_oracle_sample(wl, n, cores)
+        tot_p += p
+        tot_t += t
+    v = tot_p / tot_t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "sweep: 4096 speeds 3000-30000 rpm, 4-flute D10, 3+3 modes, "
+                               "10 um runout, [0.05,15] x 10, 60 revs, 40 slices",
+                   "sample_points_per_step": n},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n} seeded sweep points per step; the reference is "
+                                   f"JavaScript with no JS runtime on this box, so its C++ "
+                                   f"FP64 restatement runs, {cores} threads, {cpu_model()}"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def ours(args) -> int:
+    import torch
+
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=timedelta(seconds=120))
+    device = local if torch.cuda.is_available() else 0
+    torch.cuda.set_device(device)
+    import mcs
+    from mcs import workloads as W
+
+    wl = W.sweep(seed=1 + rank)
+    ctx = mcs.Context(device)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+
+    plan = ctx.plan(wl.setups, wl.modals, wl.points, wl.opts)
+    info = plan.info()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def maxover(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        plan.execute()
+    res = plan.results()
+    assert np.all(res["status"] == 0), np.unique(res["status"])
+
+    # ---- value: device-resident inputs, CUDA events on the launching stream ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)  # write 256 MiB (> 126 MB L2) between timed steps
+            starts[i].record(stream)
+            plan.execute()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = maxover(float(np.sum(step_ms))) / args.steps
+    res = plan.results()
+    pts_total = wl.n * world
+    value = pts_total / (ms / 1e3)
+
+    # algorithmic work of one step (same inputs every step): the reference loop's
+    # evaluations, in cut and out of cut
+    evals = float(res["evals"].sum())
+    engaged = float(res["engaged"].sum())
+    flop = FLOP_ENGAGED * engaged + FLOP_IDLE * (evals - engaged)
+    achieved_tflops = flop / (float(np.mean(step_ms)) / 1e3) / 1e12
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    f_mhz = clocks["sm_mhz"] or 1965.0
+    peak_tflops = sms * 128 * 2 * f_mhz * 1e6 / 1e12
+
+    # ---- e2e: public blocking API from page-locked host buffers ----
+    def pinned(arr):
+        t = torch.empty(arr.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(arr.dtype)
+        v[:] = arr
+        return t, v
+
+    keep = []
+    hs = [pinned(wl.setups), pinned(wl.modals), pinned(wl.points)]
+    keep += hs
+    from mcs import _abi as A
+    out_t = torch.empty(len(wl.points) * A.RESULT_DTYPE.itemsize, dtype=torch.uint8,
+                        pin_memory=True)
+    out_v = out_t.numpy().view(A.RESULT_DTYPE)
+    import ctypes as C
+
+    L = ctx._L
+    args_c = (ctx._h, C.c_void_p(hs[0][1].ctypes.data), len(wl.setups),
+              C.c_void_p(hs[1][1].ctypes.data), len(wl.modals),
+              C.c_void_p(hs[2][1].ctypes.data), len(wl.points), C.byref(wl.opts),
+              C.c_void_p(out_v.ctypes.data))
+    for _ in range(max(1, args.warmup // 2)):
+        mcs._lib.check(L.mcs_solve(*args_c))
+    e2e_steps = max(2, min(args.steps, 5))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        mcs._lib.check(L.mcs_solve(*args_c))
+    torch.cuda.synchronize()
+    e2e_s = maxover(time.perf_counter() - t0) / e2e_steps
+    barrier()
+    assert np.array_equal(out_v["alim"], res["alim"]), "e2e and plan results differ"
+
+    line = None
+    if rank == 0:
+        cpu = cpu_baseline(wl) if world == 1 and not args.no_cpu else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded sweep; no public dataset exists for this path)",
+            "config": {"workload": "sweep: 4096 speeds 3000-30000 rpm, 4-flute D10 helix 30, "
+                                   "3+3 modes, 10 um runout, [0.05,15] x 10, 60 revs, 40 slices",
+                       "points_per_gpu": wl.n, "variant": "plain GPU bisection",
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "kernels_per_step": info["kernels"], "graph": bool(info["graph"]),
+                       "blocks": info["blocks"], "smem_per_warp_max": info["smem_per_warp"]},
+            "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops,
+                         "unit": "TFLOP/s", "frac": achieved_tflops / peak_tflops,
+                         "traffic": None,
+                         "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 flop x "
+                                        f"{f_mhz:.0f} MHz sampled SM clock (no FP32 figure "
+                                        "in MEASURED_PEAKS.json)",
+                         "work": f"{FLOP_ENGAGED:.0f} flop per in-cut and {FLOP_IDLE:.0f} per "
+                                 f"out-of-cut reference evaluation; {evals:.3e} evaluations, "
+                                 f"{engaged:.3e} in cut per step"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": pts_total / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": int(info["h2d_bytes"]),
+                    "d2h_bytes_per_step": int(info["d2h_bytes"])},
+            "gpu_launches": int(info["kernels"]) * args.steps,
+            "clocks": clocks,
+            "results": {"open": int(res["open"].sum()), "alim_median": float(np.median(res["alim"]))},
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    a = ap.parse_args(argv)
+    if a.warmup < 3:
+        a.warmup = 3
+    if a.impl == "reference":
+        return reference_arm(a)
+    return ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,239 @@
+/*
+ * mcs.h -- C ABI of libmcs.so, the B200 (sm_100a) time-domain regenerative-chatter
+ * stability library.
+ *
+ * The library replaces the JavaScript hot path of the machining simulator:
+ *   - chatterAt / timeDomainLimit          src/stabtd.js:14-32
+ *   - the CuttingEngine force law, modal
+ *     integration and chatter index they
+ *     run per trial                         src/cutting.js:39-124,146-296,299-318
+ *   - the stability Web Worker's sweep     src/stabworker.js:6-14
+ *   - zero-order lobes / alimAt            src/sld.js:6-76
+ *
+ * All inputs and outputs are caller-owned host arrays of the plain structs below
+ * (structure-of-records, no pointers inside).  Units follow the reference engine:
+ * lengths in mm, modal stiffness in N/mm, frequencies in Hz, runout in mm.
+ * Every entry point returns an mcs_status; on failure mcs_last_error() holds a
+ * message for the calling thread.  There is no CPU fallback: without a CUDA device
+ * the calls fail with MCS_ERR_CUDA.
+ *
+ * Thread safety: a context may be shared between threads; calls on one context are
+ * serialised by a mutex inside it.
+ */
+#ifndef MCS_H_
+#define MCS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCS_ABI_VERSION 1
+#define MCS_MAX_MODES 4 /* modes per axis (frf.js fitModes keeps at most 4) */
+#define MCS_MAX_TEETH 8
+#define MCS_BINS 180    /* angular bins of the engagement map, cutting.js:15 */
+
+typedef enum {
+  MCS_OK = 0,
+  MCS_ERR_ARG = 1,         /* invalid argument (sizes, indices, NaN, out-of-range values) */
+  MCS_ERR_CUDA = 2,        /* CUDA runtime error or no device */
+  MCS_ERR_TIMEOUT = 3,     /* a bounded device wait gave up */
+  MCS_ERR_DIVERGED = 4,    /* NaN/Inf in a simulated trial (per point) */
+  MCS_ERR_CANCELLED = 5,   /* the job was cancelled before this point ran */
+  MCS_ERR_NOMEM = 6,       /* allocation failed */
+  MCS_ERR_UNSUPPORTED = 7, /* a case the kernels do not handle (e.g. > 64 slices) */
+  MCS_ERR_STATE = 8        /* call out of order (e.g. results of a plan never run) */
+} mcs_status;
+
+typedef enum { MCS_TOOL_FLAT = 0, MCS_TOOL_BALL = 1 } mcs_tool_type;
+
+/* One mode of the tool tip: frf.js:1-11 {k [N/mm], fn [Hz], zeta}. */
+typedef struct {
+  double k;
+  double fn;
+  double zeta;
+} mcs_mode;
+
+/* Modal set of the tool tip, frf.js modeSet: ny == 0 means y takes the x modes. */
+typedef struct {
+  int32_t nx;
+  int32_t ny;
+  mcs_mode x[MCS_MAX_MODES];
+  mcs_mode y[MCS_MAX_MODES];
+} mcs_modal;
+
+/* Tool as CuttingEngine.configure reads it (cutting.js:39-44). */
+typedef struct {
+  int32_t N;           /* flutes, 1..MCS_MAX_TEETH */
+  int32_t type;        /* mcs_tool_type */
+  double R;            /* radius [mm] */
+  double helix_deg;    /* helix angle [deg] */
+  double flute_len;    /* flute length [mm] */
+  double runout;       /* radial runout e [mm] */
+  double runout_phase; /* runout phase gamma [rad] */
+} mcs_tool;
+
+/* Cutting coefficients, materials.js:2-14 (Kac/Kae act only on Fz and are not needed). */
+typedef struct {
+  double Ktc, Krc; /* shearing [N/mm^2] */
+  double Kte, Kre; /* edge [N/mm] */
+  double mc;       /* size-effect exponent */
+  double Ci;       /* process-damping coefficient [N/m] */
+} mcs_material;
+
+/* Everything of a cut except the speed and the modes. */
+typedef struct {
+  mcs_tool tool;
+  mcs_material mat;
+  double arc_st, arc_ex; /* engagement arc [rad], identify.js immersion() */
+  double fz;             /* feed per tooth [mm] */
+} mcs_setup;
+
+/* One boundary point: a setup at a spindle speed with the modal set at that speed
+ * (the Worker message carries one modal per point, stabworker.js:10 / main.js:496). */
+typedef struct {
+  uint32_t setup;
+  uint32_t modal;
+  double S; /* spindle speed [rpm] */
+} mcs_point;
+
+/* Options of timeDomainLimit/chatterAt (stabtd.js:14,24) plus explicit overrides. */
+typedef struct {
+  double a_min, a_max;     /* bisection range [mm] (reference 0.05, 20) */
+  int32_t iters;           /* bisection iterations (reference 8) */
+  int32_t revs;            /* revolutions per trial (reference 120) */
+  int32_t nonlinear;       /* size effect + process damping (reference 1) */
+  int32_t honor_runout;    /* 0: runout forced to 0 as chatterAt does (stabtd.js:16) */
+  int32_t steps_per_tooth; /* 0: reference rule max(48, ceil(Ttooth*fTop*24)) */
+  int32_t slices;          /* 0: reference rule dz = max(0.25, fluteLen/48) */
+  double chatter_idx;      /* decision threshold (reference 0.45, stabtd.js:10) */
+} mcs_opts;
+
+/* Result of timeDomainLimit for one point. */
+typedef struct {
+  double alim;          /* critical depth [mm] */
+  double lo, hi;        /* bracket [stable, chatter]; hi = +inf when open */
+  int32_t open;         /* 1 when stable at a_max (bracket[1] === Infinity) */
+  int32_t status;       /* mcs_status of this point */
+  int32_t trials;       /* trials run */
+  int32_t steps_per_tooth;
+  uint64_t evals;       /* reference-loop slice evaluations (steps * N * nz summed) */
+  uint64_t engaged;     /* of which in cut (force evaluated) */
+} mcs_result;
+
+/* One chatterAt trial: a point at an axial depth. */
+typedef struct {
+  uint32_t point;
+  uint32_t pad;
+  double ap; /* [mm] */
+} mcs_trial;
+
+/* chatterIndex() of one trial (cutting.js:299-318) and the decision. */
+typedef struct {
+  double index;
+  double once; /* sOnce [um] */
+  double amp;  /* sAll [um] */
+  int32_t chatter;
+  int32_t status;
+} mcs_trial_result;
+
+/* Zero-order lobe query, the argument object of stabilityLobes (sld.js:23). */
+typedef struct {
+  int32_t N;
+  int32_t lobes;
+  double Ktc, Krc;
+  double phi_st, phi_ex;
+  double rpm_min, rpm_max;
+  uint32_t modal; /* index into modals */
+  uint32_t pad;
+} mcs_lobe_query;
+
+/* Launch and work figures of a plan, for measurement. */
+typedef struct {
+  int32_t blocks;        /* persistent CTAs launched */
+  int32_t warps_per_sm;  /* resident warps per SM */
+  int32_t smem_per_warp; /* bytes */
+  int32_t slots;         /* slices per lane (1 or 2) */
+  int32_t modes;         /* modes per axis the kernel was built for */
+  int32_t graph;         /* 1 when the launch is a captured CUDA graph */
+  int32_t kernels;       /* kernel launches per execute */
+  int32_t pad;
+  uint64_t n_points;
+  uint64_t h2d_bytes; /* bytes a solve of these inputs copies host -> device */
+  uint64_t d2h_bytes; /* bytes of results copied device -> host */
+} mcs_plan_info;
+
+typedef struct mcs_ctx mcs_ctx;
+typedef struct mcs_plan mcs_plan;
+typedef struct mcs_job mcs_job;
+
+/* Reference defaults of timeDomainLimit: [0.05, 20] x 8, 120 revs, nonlinear, 0.45. */
+void mcs_default_opts(mcs_opts* opts);
+
+/* Message of the last failing call made by this thread ("" if none). */
+const char* mcs_last_error(void);
+
+/* Context on one CUDA device: owns a stream, device buffers and the tuned launch shapes. */
+int mcs_create(mcs_ctx** ctx, int device);
+int mcs_destroy(mcs_ctx* ctx);
+/* The context's cudaStream_t (as void*), for callers that time or order work on it. */
+void* mcs_stream(mcs_ctx* ctx);
+
+/*
+ * Batched timeDomainLimit (stabtd.js:24-32) over n_points points -- the whole Worker
+ * sweep (stabworker.js:6-14) in one call.  Blocking: host inputs are copied to the
+ * device, every point is solved in one persistent launch and the results are copied
+ * back into out[n_points].
+ */
+int mcs_solve(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+              size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* opts,
+              mcs_result* out);
+
+/*
+ * Batched chatterAt (stabtd.js:14-22): one trial per entry of trials[], returning the
+ * chatter index parts and the decision.  Used to replay decisions at given depths.
+ */
+int mcs_chatter_at(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,
+                   const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                   size_t n_points, const mcs_trial* trials, size_t n_trials,
+                   const mcs_opts* opts, mcs_trial_result* out);
+
+/*
+ * Plans: the inputs of mcs_solve uploaded once and the launch captured in a CUDA graph,
+ * so that repeated executions run from device-resident inputs.
+ */
+int mcs_plan_create(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,
+                    const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                    size_t n_points, const mcs_opts* opts, mcs_plan** plan);
+int mcs_plan_execute(mcs_plan* plan); /* asynchronous on mcs_stream(ctx) */
+int mcs_plan_results(mcs_plan* plan, mcs_result* out); /* waits, copies results to host */
+int mcs_plan_info_get(const mcs_plan* plan, mcs_plan_info* info);
+int mcs_plan_destroy(mcs_plan* plan);
+
+/*
+ * Asynchronous solve with cancellation, the Worker's job protocol (stabworker.js:7-9):
+ * a cancelled job stops at the next trial boundary of each point; points not finished
+ * get status MCS_ERR_CANCELLED.  out must stay valid until mcs_job_wait returns.
+ */
+int mcs_solve_async(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,
+                    const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                    size_t n_points, const mcs_opts* opts, mcs_result* out, mcs_job** job);
+int mcs_job_poll(mcs_job* job, size_t* points_done, int* finished);
+int mcs_job_cancel(mcs_job* job);
+int mcs_job_wait(mcs_job* job); /* MCS_OK, or MCS_ERR_CANCELLED when cancelled */
+void mcs_job_free(mcs_job* job);
+
+/*
+ * Zero-order lobes (sld.js:23-61) read at spindle speeds (alimAt, sld.js:64-76):
+ * alim[q * n_rpm + r] for query q at rpm[r]; +inf where no lobe covers the speed.
+ */
+int mcs_lobes_alim(mcs_ctx* ctx, const mcs_modal* modals, size_t n_modals,
+                   const mcs_lobe_query* queries, size_t n_queries, const double* rpm,
+                   size_t n_rpm, double* alim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCS_H_ */

@@ -1,0 +1,924 @@
+// C ABI of libmcs.so (include/mcs.h): input validation, per-point preparation on the
+// host (the FP64 derivations of CuttingEngine.configure, src/cutting.js:39-82), work
+// ordering and bucketing, CUDA-graph plans, blocking and asynchronous solves.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "mcs_internal.h"
+
+using namespace mcs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define MCS_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(MCS_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));         \
+  } while (0)
+
+constexpr double kPi = 3.141592653589793;
+constexpr int kMaxBuckets = 8;
+
+inline bool is_finite(double v) { return std::isfinite(v); }
+
+// ------------------------------------------------------------------ validation
+int check_inputs(const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+                 size_t n_modals, const mcs_point* points, size_t n_points,
+                 const mcs_opts* o) {
+  if (!o) return fail(MCS_ERR_ARG, "opts is NULL");
+  if (n_points && (!setups || !modals || !points))
+    return fail(MCS_ERR_ARG, "NULL input array");
+  if (n_points > (size_t)std::numeric_limits<int32_t>::max())
+    return fail(MCS_ERR_ARG, "too many points (%zu)", n_points);
+  if (!(is_finite(o->a_min) && is_finite(o->a_max) && o->a_min > 0 && o->a_max >= o->a_min))
+    return fail(MCS_ERR_ARG, "bisection range must satisfy 0 < a_min <= a_max");
+  if (o->iters < 0 || o->iters > 60) return fail(MCS_ERR_ARG, "iters out of range [0, 60]");
+  if (o->revs < 1 || o->revs > 1000000) return fail(MCS_ERR_ARG, "revs out of range");
+  if (o->steps_per_tooth < 0 || o->steps_per_tooth > 10000000)
+    return fail(MCS_ERR_ARG, "steps_per_tooth out of range");
+  if (o->slices < 0) return fail(MCS_ERR_ARG, "slices must be >= 0");
+  if (o->slices > kMaxSlots * kWarp)
+    return fail(MCS_ERR_UNSUPPORTED, "at most %d slices are supported", kMaxSlots * kWarp);
+  if (!is_finite(o->chatter_idx)) return fail(MCS_ERR_ARG, "chatter_idx is not finite");
+  for (size_t i = 0; i < n_setups; i++) {
+    const mcs_setup& s = setups[i];
+    const mcs_tool& t = s.tool;
+    if (t.N < 1 || t.N > kMaxTeeth)
+      return fail(MCS_ERR_ARG, "setup %zu: N must be in [1, %d]", i, kMaxTeeth);
+    if (t.type != MCS_TOOL_FLAT && t.type != MCS_TOOL_BALL)
+      return fail(MCS_ERR_ARG, "setup %zu: unknown tool type", i);
+    if (!(is_finite(t.R) && t.R > 0)) return fail(MCS_ERR_ARG, "setup %zu: R must be > 0", i);
+    if (!(is_finite(t.helix_deg) && std::fabs(t.helix_deg) < 89))
+      return fail(MCS_ERR_ARG, "setup %zu: helix out of range", i);
+    if (!(is_finite(t.flute_len) && t.flute_len > 0))
+      return fail(MCS_ERR_ARG, "setup %zu: flute_len must be > 0", i);
+    if (!(is_finite(t.runout) && is_finite(t.runout_phase)))
+      return fail(MCS_ERR_ARG, "setup %zu: runout not finite", i);
+    const mcs_material& m = s.mat;
+    if (!(is_finite(m.Ktc) && is_finite(m.Krc) && is_finite(m.Kte) && is_finite(m.Kre) && is_finite(m.mc) &&
+          is_finite(m.Ci) && m.mc >= 0 && m.Ci >= 0))
+      return fail(MCS_ERR_ARG, "setup %zu: material coefficients invalid", i);
+    if (!(is_finite(s.fz) && s.fz > 0)) return fail(MCS_ERR_ARG, "setup %zu: fz must be > 0", i);
+    if (!(is_finite(s.arc_st) && is_finite(s.arc_ex)))
+      return fail(MCS_ERR_ARG, "setup %zu: arc not finite", i);
+  }
+  for (size_t i = 0; i < n_modals; i++) {
+    const mcs_modal& md = modals[i];
+    if (md.nx < 1 || md.nx > kMaxModes || md.ny < 0 || md.ny > kMaxModes)
+      return fail(MCS_ERR_ARG, "modal %zu: 1 <= nx <= %d and 0 <= ny <= %d", i, kMaxModes,
+                  kMaxModes);
+    for (int a = 0; a < 2; a++) {
+      const int cnt = a == 0 ? md.nx : md.ny;
+      const mcs_mode* ms = a == 0 ? md.x : md.y;
+      for (int j = 0; j < cnt; j++)
+        if (!(is_finite(ms[j].k) && ms[j].k > 0 && is_finite(ms[j].fn) && ms[j].fn > 0 &&
+              is_finite(ms[j].zeta) && ms[j].zeta >= 0))
+          return fail(MCS_ERR_ARG, "modal %zu: mode %d needs k > 0, fn > 0, zeta >= 0", i, j);
+    }
+  }
+  for (size_t i = 0; i < n_points; i++) {
+    const mcs_point& p = points[i];
+    if (p.setup >= n_setups) return fail(MCS_ERR_ARG, "point %zu: setup index out of range", i);
+    if (p.modal >= n_modals) return fail(MCS_ERR_ARG, "point %zu: modal index out of range", i);
+    if (!(is_finite(p.S) && p.S > 0)) return fail(MCS_ERR_ARG, "point %zu: S must be > 0", i);
+  }
+  return MCS_OK;
+}
+
+// ------------------------------------------------------------------ preparation
+// Slices a trial at depth ap uses (setEngagement with chatterAt's fluteLen).
+int slices_at(double ap, double flute_len, int override_n) {
+  if (ap <= 0) return 0;
+  if (override_n > 0) return override_n;
+  const double flute = std::max(flute_len, ap + 1.0);
+  const double dz = std::max(0.25, flute / 48.0);
+  const int maxs = (int)std::ceil(flute / dz);
+  return std::min(maxs, (int)std::ceil(ap / dz));
+}
+
+struct Prepared {
+  PointParams pp;
+  double cost;
+  int modes;  // max modes per axis
+};
+
+int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const mcs_opts& o,
+                  double ap_max, Prepared& out) {
+  PointParams& P = out.pp;
+  std::memset(&P, 0, sizeof(P));
+  const mcs_tool& t = st.tool;
+  const int N = t.N;
+  const double S = std::max(100.0, S_in);
+  const double omega = S * 2 * kPi / 60;
+  const double Ttooth = 60 / (S * N);
+  const int nx = md.nx, ny = md.ny > 0 ? md.ny : md.nx;
+  const mcs_mode* xm = md.x;
+  const mcs_mode* ym = md.ny > 0 ? md.y : md.x;
+  double fTop = -INFINITY;
+  for (int j = 0; j < nx; j++) fTop = std::max(fTop, xm[j].fn);
+  for (int j = 0; j < ny; j++) fTop = std::max(fTop, ym[j].fn);
+  // steps per tooth period: 24 per period of the highest mode, at least 48 (cutting.js:50)
+  double sptd = o.steps_per_tooth > 0 ? (double)o.steps_per_tooth
+                                      : std::max(48.0, std::ceil(Ttooth * fTop * 24));
+  const double nsteps_d = sptd * N * (double)o.revs;
+  if (sptd * N > 1e7 || nsteps_d >= 2147483647.0)
+    return fail(MCS_ERR_UNSUPPORTED, "trial of %.0f steps is too long for the kernels", nsteps_d);
+  const int spt = (int)sptd;
+  const double dt = Ttooth / spt;
+  P.omega = omega;
+  P.dphi = omega * dt;
+  P.R = t.R;
+  P.tanB = std::tan(t.helix_deg * kPi / 180);
+  P.flute_len = t.flute_len;
+  P.Ci = o.nonlinear ? st.mat.Ci : 0.0;
+  P.fz = (float)st.fz;
+  P.hmax = (float)std::max(0.1, 3 * st.fz);
+  P.Ktc = (float)st.mat.Ktc;
+  P.Krc = (float)st.mat.Krc;
+  P.Kte = (float)st.mat.Kte;
+  P.Kre = (float)st.mat.Kre;
+  P.mc = o.nonlinear ? (float)st.mat.mc : 0.f;
+  P.dtf = (float)dt;
+  // runout offsets delta_i = e cos(2 pi i / N - gamma) (cutting.js:44); chatterAt uses 0
+  for (int i = 0; i < N; i++)
+    P.dR[i] = o.honor_runout ? (float)(t.runout * std::cos(2 * kPi * i / N - t.runout_phase))
+                             : 0.f;
+  // modes: k [N/m], m = k / (2 pi fn)^2, c = 2 zeta sqrt(k m) (cutting.js:54-59)
+  for (int a = 0; a < 2; a++) {
+    const int cnt = a == 0 ? nx : ny;
+    const mcs_mode* ms = a == 0 ? xm : ym;
+    for (int j = 0; j < cnt; j++) {
+      const double k = ms[j].k * 1e3;
+      const double w = 2 * kPi * ms[j].fn;
+      const double m = k / (w * w);
+      const double c = 2 * ms[j].zeta * std::sqrt(k * m);
+      P.mk[a][j] = (float)k;
+      P.mcd[a][j] = (float)c;
+      P.ma[a][j] = (float)(dt / m);
+    }
+  }
+  out.modes = std::max(nx, ny);
+  P.N = N;
+  P.spt = spt;
+  P.spr = N * spt;
+  P.decim = (int)std::max(1.0, std::floor(spt / 40.0 + 0.5));
+  P.nsteps = (int)nsteps_d;
+  P.type = t.type;
+  P.slices_override = o.slices;
+  // engaged bins of the static map chatterAt builds (stabtd.js:17): bin b is in the
+  // arc when its centre (b + 0.5)/180*2pi lies in [arc_st, arc_ex]
+  int b0 = -1, b1 = -1;
+  for (int b = 0; b < MCS_BINS; b++) {
+    const double phi = (b + 0.5) / MCS_BINS * 2 * kPi;
+    if (phi >= st.arc_st && phi <= st.arc_ex) {
+      if (b0 < 0) b0 = b;
+      b1 = b;
+    }
+  }
+  const double binScale = MCS_BINS / (2 * kPi);
+  P.empty = b0 < 0 ? 1 : 0;
+  if (!P.empty) {
+    P.phi_lo = b0 / binScale;
+    // sin(phi) <= 0 is out of cut (cutting.js:190): nothing at or past pi
+    P.phi_hi = std::min((b1 + 1) / binScale, kPi);
+    P.excl_zero = b0 == 0 ? 1 : 0;
+    if (P.phi_hi <= P.phi_lo) P.empty = 1;
+  }
+  const double span = P.empty ? 0.0 : P.phi_hi - P.phi_lo;
+  const int lmax = P.empty ? 1 : (int)std::floor(span / P.dphi) + 2;
+  P.lpad = std::min(lmax, P.spr) | 1;
+  P.nz_max = slices_at(ap_max, t.flute_len, o.slices);
+  if (P.nz_max > kMaxSlots * kWarp)
+    return fail(MCS_ERR_UNSUPPORTED, "%d slices exceed the %d the kernels support", P.nz_max,
+                kMaxSlots * kWarp);
+  // chatter-index windows (cutting.js:301,310): the last n tooth samples and the last
+  // m = round(n spt / decim) history samples
+  const long long C = (long long)N * o.revs;
+  P.ts_n = (int)std::min<long long>(C, 24);
+  P.ts_c0 = (int)(C - P.ts_n);
+  const long long H = (long long)P.nsteps / P.decim;
+  P.hist_m = (int)std::min<long long>(H, (long long)std::floor((double)P.ts_n * spt / P.decim + 0.5));
+  P.hist_h0 = (int)(H - P.hist_m);
+  const long long smem = (long long)((P.spr * 8 + 15) & ~15) + 4LL * P.nz_max * P.lpad;
+  if (smem > kMaxSmemPerWarp)
+    return fail(MCS_ERR_UNSUPPORTED,
+                "point needs %lld bytes of shared memory (spr %d, %d slices): above %d", smem,
+                P.spr, P.nz_max, kMaxSmemPerWarp);
+  P.smem_bytes = (int)smem;
+  // relative cost for ordering: steps x (visited teeth x slots + fixed per-step work)
+  const double lag_span = std::fabs(ap_max * P.tanB / P.R);
+  const double act = std::min(1.0, (span + lag_span) / (2 * kPi) + 1.0 / N);
+  const int slots = (P.nz_max + kWarp - 1) / kWarp;
+  out.cost = (double)P.nsteps * (o.iters + 1) * (24.0 + 40.0 * N * std::max(1, slots) * act);
+  return MCS_OK;
+}
+
+int slots_for(int nz) { return nz <= kWarp ? 1 : 2; }
+
+// ------------------------------------------------------------------ device buffers
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return MCS_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(e == cudaErrorMemoryAllocation ? MCS_ERR_NOMEM : MCS_ERR_CUDA,
+                  "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+    }
+    cap = want;
+    return MCS_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct Bucket {
+  KernelShape shape;
+  int smem = 0;
+  int grid = 0;
+  int offset = 0;  // into the order array
+  int count = 0;
+  int blocks_per_sm = 0;
+};
+
+}  // namespace
+
+struct mcs_ctx {
+  int device = 0;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t aux[kMaxBuckets] = {};
+  cudaStream_t side = nullptr;  // progress reads and cancellation while a job runs
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kMaxBuckets] = {};
+  std::mutex mu;
+  void* pinned = nullptr;  // upload staging (page-locked), grown on demand
+  size_t pinned_cap = 0;
+};
+
+struct mcs_plan {
+  mcs_ctx* ctx = nullptr;
+  size_t n = 0;
+  bool trials = false;
+  std::vector<Bucket> buckets;
+  DevBuf params, order, results, queues, items;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int max_modes = 1;
+  int max_slots = 1;
+  bool executed = false;
+};
+
+struct mcs_job {
+  mcs_plan* plan = nullptr;
+  mcs_result* out = nullptr;
+  mcs_result* staging = nullptr;  // pinned
+  DevBuf cancel, progress;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  bool waited = false;
+};
+
+namespace {
+
+// Orders the work items by cost (largest first) and groups them into buckets of similar
+// shared-memory need, each launched as its own persistent grid.
+int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
+                 const std::vector<int>& slots, const std::vector<int>& modes, bool trials,
+                 std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
+  const size_t n = smem.size();
+  std::vector<int32_t> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return smem[a] > smem[b]; });
+  buckets.clear();
+  order.clear();
+  order.reserve(n);
+  if (n == 0) return MCS_OK;
+  const double hi = smem[idx.front()], lo = std::max(1, smem[idx.back()]);
+  const double ratio = std::max(1.3, std::pow(hi / lo, 1.0 / kMaxBuckets) * 1.0001);
+  size_t i = 0;
+  while (i < n) {
+    Bucket b;
+    const int top = smem[idx[i]];
+    size_t j = i;
+    int sl = 1, nm = 1;
+    while (j < n && (double)smem[idx[j]] * ratio >= top) {
+      sl = std::max(sl, slots[idx[j]]);
+      nm = std::max(nm, modes[idx[j]]);
+      j++;
+    }
+    if ((int)buckets.size() == kMaxBuckets - 1) {  // last bucket takes the rest
+      for (size_t k = j; k < n; k++) {
+        sl = std::max(sl, slots[idx[k]]);
+        nm = std::max(nm, modes[idx[k]]);
+      }
+      j = n;
+    }
+    std::vector<int32_t> seg(idx.begin() + i, idx.begin() + j);
+    std::stable_sort(seg.begin(), seg.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+    b.offset = (int)order.size();
+    b.count = (int)seg.size();
+    b.smem = (top + 15) & ~15;
+    b.shape = KernelShape{sl, nm};
+    order.insert(order.end(), seg.begin(), seg.end());
+    int bps = 0;
+    const int rc = trials ? occupancy_trials(b.shape, b.smem, &bps)
+                          : occupancy_solve(b.shape, b.smem, &bps);
+    if (rc != 0)
+      return fail(MCS_ERR_CUDA, "occupancy query failed: %s",
+                  cudaGetErrorString((cudaError_t)rc));
+    if (bps < 1)
+      return fail(MCS_ERR_UNSUPPORTED, "a %d-byte warp does not fit on an SM", b.smem);
+    b.blocks_per_sm = bps;
+    b.grid = (int)std::min<long long>(b.count, (long long)bps * ctx->sms);
+    buckets.push_back(b);
+    i = j;
+  }
+  return MCS_OK;
+}
+
+DevOpts dev_opts(const mcs_opts* o) {
+  DevOpts d;
+  d.a_min = o->a_min;
+  d.a_max = o->a_max;
+  d.chatter_idx = o->chatter_idx;
+  d.iters = o->iters;
+  d.pad = 0;
+  return d;
+}
+
+// Enqueue the plan's work: zero the queue counters, fork one stream per bucket, join.
+int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int* cancel,
+            unsigned int* progress, double chatter_idx) {
+  mcs_ctx* ctx = pl->ctx;
+  const int nb = (int)pl->buckets.size();
+  MCS_CUDA(cudaMemsetAsync(pl->queues.p, 0, sizeof(unsigned int) * std::max(1, nb), s0));
+  if (progress) MCS_CUDA(cudaMemsetAsync(progress, 0, sizeof(unsigned int), s0));
+  if (nb == 0) return MCS_OK;
+  MCS_CUDA(cudaEventRecord(ctx->fork, s0));
+  for (int b = 0; b < nb; b++) {
+    const Bucket& bk = pl->buckets[b];
+    cudaStream_t sb = nb == 1 ? s0 : ctx->aux[b];
+    if (sb != s0) MCS_CUDA(cudaStreamWaitEvent(sb, ctx->fork, 0));
+    unsigned int* q = static_cast<unsigned int*>(pl->queues.p) + b;
+    const int32_t* order = static_cast<const int32_t*>(pl->order.p) + bk.offset;
+    int rc;
+    if (pl->trials)
+      rc = launch_trials(bk.shape, bk.grid, bk.smem, sb,
+                         static_cast<const PointParams*>(pl->params.p),
+                         static_cast<const TrialItem*>(pl->items.p) + bk.offset, bk.count,
+                         chatter_idx, static_cast<mcs_trial_result*>(pl->results.p), q);
+    else
+      rc = launch_solve(bk.shape, bk.grid, bk.smem, sb,
+                        static_cast<const PointParams*>(pl->params.p), order, bk.count,
+                        dev_opts(o), static_cast<mcs_result*>(pl->results.p), q, cancel,
+                        progress);
+    if (rc != 0)
+      return fail(MCS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+    if (sb != s0) {
+      MCS_CUDA(cudaEventRecord(ctx->join[b], sb));
+      MCS_CUDA(cudaStreamWaitEvent(s0, ctx->join[b], 0));
+    }
+  }
+  return MCS_OK;
+}
+
+void plan_free(mcs_plan* pl) {
+  if (!pl) return;
+  if (pl->exec) cudaGraphExecDestroy(pl->exec);
+  if (pl->graph) cudaGraphDestroy(pl->graph);
+  pl->params.release();
+  pl->order.release();
+  pl->results.release();
+  pl->queues.release();
+  pl->items.release();
+  delete pl;
+}
+
+// Copies two host arrays to the device through the context's page-locked staging buffer
+// and waits for the copies (the staging buffer is reused by the next call).
+int upload2(mcs_ctx* ctx, cudaStream_t stream, void* d1, const void* h1, size_t n1, void* d2,
+            const void* h2, size_t n2) {
+  const size_t off2 = (n1 + 255) & ~size_t(255);
+  const size_t need = off2 + n2;
+  if (need > ctx->pinned_cap) {
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_cap = 0;
+    const size_t want = std::max<size_t>(need, 1 << 20);
+    cudaError_t e = cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      ctx->pinned = nullptr;
+      return fail(MCS_ERR_NOMEM, "cudaHostAlloc(%zu) failed: %s", want, cudaGetErrorString(e));
+    }
+    ctx->pinned_cap = want;
+  }
+  char* st = static_cast<char*>(ctx->pinned);
+  std::memcpy(st, h1, n1);
+  if (n2) std::memcpy(st + off2, h2, n2);
+  MCS_CUDA(cudaMemcpyAsync(d1, st, n1, cudaMemcpyHostToDevice, stream));
+  if (n2) MCS_CUDA(cudaMemcpyAsync(d2, st + off2, n2, cudaMemcpyHostToDevice, stream));
+  MCS_CUDA(cudaStreamSynchronize(stream));
+  return MCS_OK;
+}
+
+// Validates, prepares and uploads a solve batch; optionally captures it in a graph.
+int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+               size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* o,
+               bool capture, cudaStream_t stream, mcs_plan** out) {
+  int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
+  if (rc) return rc;
+  std::vector<PointParams> pp(n_points);
+  std::vector<int> smem(n_points), slots(n_points), modes(n_points);
+  std::vector<double> cost(n_points);
+  for (size_t i = 0; i < n_points; i++) {
+    Prepared pr;
+    rc = prepare_point(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,
+                       o->a_max, pr);
+    if (rc) return fail(rc, "point %zu: %s", i, g_last_error.c_str());
+    pp[i] = pr.pp;
+    smem[i] = pr.pp.smem_bytes;
+    slots[i] = slots_for(pr.pp.nz_max);
+    modes[i] = pr.modes;
+    cost[i] = pr.cost;
+  }
+  mcs_plan* pl = new mcs_plan();
+  pl->ctx = ctx;
+  pl->n = n_points;
+  std::vector<int32_t> order;
+  rc = make_buckets(ctx, smem, cost, slots, modes, false, order, pl->buckets);
+  if (rc) {
+    plan_free(pl);
+    return rc;
+  }
+  const size_t nb = std::max<size_t>(1, pl->buckets.size());
+  if ((rc = pl->params.ensure(sizeof(PointParams) * std::max<size_t>(1, n_points))) ||
+      (rc = pl->order.ensure(sizeof(int32_t) * std::max<size_t>(1, n_points))) ||
+      (rc = pl->results.ensure(sizeof(mcs_result) * std::max<size_t>(1, n_points))) ||
+      (rc = pl->queues.ensure(sizeof(unsigned int) * nb))) {
+    plan_free(pl);
+    return rc;
+  }
+  if (n_points) {
+    rc = upload2(ctx, stream, pl->params.p, pp.data(), sizeof(PointParams) * n_points,
+                 pl->order.p, order.data(), sizeof(int32_t) * n_points);
+    if (rc) {
+      plan_free(pl);
+      return rc;
+    }
+  }
+  for (const Bucket& b : pl->buckets) {
+    pl->max_modes = std::max(pl->max_modes, b.shape.modes);
+    pl->max_slots = std::max(pl->max_slots, b.shape.slots);
+  }
+  if (capture) {
+    cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      plan_free(pl);
+      return fail(MCS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    }
+    rc = enqueue(pl, stream, o, nullptr, nullptr, o->chatter_idx);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(stream, &g);
+    if (rc || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      plan_free(pl);
+      return rc ? rc : fail(MCS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    }
+    pl->graph = g;
+    e = cudaGraphInstantiate(&pl->exec, g, 0);
+    if (e != cudaSuccess) {
+      plan_free(pl);
+      return fail(MCS_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+    }
+  }
+  *out = pl;
+  return MCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mcs_default_opts(mcs_opts* o) {
+  if (!o) return;
+  o->a_min = 0.05;
+  o->a_max = 20.0;
+  o->iters = 8;
+  o->revs = 120;
+  o->nonlinear = 1;
+  o->honor_runout = 0;
+  o->steps_per_tooth = 0;
+  o->slices = 0;
+  o->chatter_idx = 0.45;
+}
+
+const char* mcs_last_error(void) { return g_last_error.c_str(); }
+
+int mcs_create(mcs_ctx** out, int device) {
+  if (!out) return fail(MCS_ERR_ARG, "ctx pointer is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(MCS_ERR_CUDA, "no CUDA device: %s",
+                e != cudaSuccess ? cudaGetErrorString(e) : "device count is 0");
+  if (device < 0 || device >= count)
+    return fail(MCS_ERR_ARG, "device %d out of range (%d devices)", device, count);
+  MCS_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  MCS_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(MCS_ERR_UNSUPPORTED, "device %d is sm_%d%d; the kernels are built for sm_100a",
+                device, prop.major, prop.minor);
+  const int rc = set_smem_limits();
+  if (rc) return fail(MCS_ERR_CUDA, "kernel attributes: %s", cudaGetErrorString((cudaError_t)rc));
+  mcs_ctx* c = new mcs_ctx();
+  c->device = device;
+  c->sms = prop.multiProcessorCount;
+  bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int b = 0; ok && b < kMaxBuckets; b++)
+    ok = cudaStreamCreateWithFlags(&c->aux[b], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->join[b], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    mcs_destroy(c);
+    return fail(MCS_ERR_CUDA, "stream/event creation failed");
+  }
+  *out = c;
+  return MCS_OK;
+}
+
+int mcs_destroy(mcs_ctx* c) {
+  if (!c) return MCS_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int b = 0; b < kMaxBuckets; b++) {
+    if (c->aux[b]) cudaStreamDestroy(c->aux[b]);
+    if (c->join[b]) cudaEventDestroy(c->join[b]);
+  }
+  if (c->fork) cudaEventDestroy(c->fork);
+  if (c->side) cudaStreamDestroy(c->side);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->pinned) cudaFreeHost(c->pinned);
+  delete c;
+  return MCS_OK;
+}
+
+void* mcs_stream(mcs_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int mcs_plan_create(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
+                    const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                    size_t n_points, const mcs_opts* opts, mcs_plan** plan) {
+  if (!c || !plan) return fail(MCS_ERR_ARG, "NULL ctx or plan pointer");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  return build_plan(c, setups, n_setups, modals, n_modals, points, n_points, opts, true,
+                    c->stream, plan);
+}
+
+int mcs_plan_execute(mcs_plan* pl) {
+  if (!pl) return fail(MCS_ERR_ARG, "plan is NULL");
+  std::lock_guard<std::mutex> lk(pl->ctx->mu);
+  MCS_CUDA(cudaSetDevice(pl->ctx->device));
+  if (pl->exec) MCS_CUDA(cudaGraphLaunch(pl->exec, pl->ctx->stream));
+  pl->executed = true;
+  return MCS_OK;
+}
+
+int mcs_plan_results(mcs_plan* pl, mcs_result* out) {
+  if (!pl || (!out && pl->n)) return fail(MCS_ERR_ARG, "NULL plan or output");
+  if (!pl->executed) return fail(MCS_ERR_STATE, "plan was never executed");
+  std::lock_guard<std::mutex> lk(pl->ctx->mu);
+  MCS_CUDA(cudaSetDevice(pl->ctx->device));
+  if (pl->n)
+    MCS_CUDA(cudaMemcpyAsync(out, pl->results.p, sizeof(mcs_result) * pl->n,
+                             cudaMemcpyDeviceToHost, pl->ctx->stream));
+  MCS_CUDA(cudaStreamSynchronize(pl->ctx->stream));
+  return MCS_OK;
+}
+
+int mcs_plan_info_get(const mcs_plan* pl, mcs_plan_info* info) {
+  if (!pl || !info) return fail(MCS_ERR_ARG, "NULL plan or info");
+  std::memset(info, 0, sizeof(*info));
+  int warps = 0, smem = 0;
+  for (const Bucket& b : pl->buckets) {
+    info->blocks += b.grid;
+    warps = std::max(warps, b.blocks_per_sm);
+    smem = std::max(smem, b.smem);
+  }
+  info->warps_per_sm = warps;
+  info->smem_per_warp = smem;
+  info->slots = pl->max_slots;
+  info->modes = pl->max_modes;
+  info->graph = pl->exec ? 1 : 0;
+  info->kernels = (int)pl->buckets.size();
+  info->n_points = pl->n;
+  info->h2d_bytes = pl->trials ? 0 : (uint64_t)pl->n * (sizeof(PointParams) + sizeof(int32_t));
+  info->d2h_bytes = pl->trials ? 0 : (uint64_t)pl->n * sizeof(mcs_result);
+  return MCS_OK;
+}
+
+int mcs_plan_destroy(mcs_plan* pl) {
+  if (!pl) return MCS_OK;
+  {
+    std::lock_guard<std::mutex> lk(pl->ctx->mu);
+    cudaSetDevice(pl->ctx->device);
+    cudaStreamSynchronize(pl->ctx->stream);
+  }
+  plan_free(pl);
+  return MCS_OK;
+}
+
+int mcs_solve(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+              size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* opts,
+              mcs_result* out) {
+  if (!c) return fail(MCS_ERR_ARG, "ctx is NULL");
+  if (n_points && !out) return fail(MCS_ERR_ARG, "out is NULL");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  mcs_plan* pl = nullptr;
+  int rc = build_plan(c, setups, n_setups, modals, n_modals, points, n_points, opts, false,
+                      c->stream, &pl);
+  if (rc) return rc;
+  rc = enqueue(pl, c->stream, opts, nullptr, nullptr, opts->chatter_idx);
+  if (!rc && n_points) {
+    cudaError_t e = cudaMemcpyAsync(out, pl->results.p, sizeof(mcs_result) * n_points,
+                                    cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "result copy failed: %s", cudaGetErrorString(e));
+  }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "solve failed: %s", cudaGetErrorString(e));
+  plan_free(pl);
+  return rc;
+}
+
+int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
+                   const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                   size_t n_points, const mcs_trial* trials, size_t n_trials,
+                   const mcs_opts* o, mcs_trial_result* out) {
+  if (!c) return fail(MCS_ERR_ARG, "ctx is NULL");
+  if (n_trials && (!trials || !out)) return fail(MCS_ERR_ARG, "NULL trials or output");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
+  if (rc) return rc;
+  if (n_trials > (size_t)std::numeric_limits<int32_t>::max())
+    return fail(MCS_ERR_ARG, "too many trials");
+  double ap_max = 0;
+  for (size_t i = 0; i < n_trials; i++) {
+    if (trials[i].point >= n_points)
+      return fail(MCS_ERR_ARG, "trial %zu: point index out of range", i);
+    if (!(is_finite(trials[i].ap) && trials[i].ap > 0 && trials[i].ap < 1e4))
+      return fail(MCS_ERR_ARG, "trial %zu: ap must be in (0, 1e4)", i);
+  }
+  // per point: the deepest trial sets its slice count
+  std::vector<double> deepest(n_points, 0.0);
+  for (size_t i = 0; i < n_trials; i++)
+    deepest[trials[i].point] = std::max(deepest[trials[i].point], trials[i].ap);
+  std::vector<PointParams> pp(n_points);
+  std::vector<int> modes(n_points);
+  for (size_t i = 0; i < n_points; i++) {
+    Prepared pr;
+    ap_max = deepest[i] > 0 ? deepest[i] : o->a_min;
+    rc = prepare_point(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,
+                       ap_max, pr);
+    if (rc) return fail(rc, "point %zu: %s", i, g_last_error.c_str());
+    pp[i] = pr.pp;
+    modes[i] = pr.modes;
+  }
+  std::vector<int> smem(n_trials), slots(n_trials), tmodes(n_trials);
+  std::vector<double> cost(n_trials);
+  std::vector<TrialItem> items_by_idx(n_trials);
+  for (size_t i = 0; i < n_trials; i++) {
+    const PointParams& P = pp[trials[i].point];
+    const int nz = slices_at(trials[i].ap, P.flute_len, o->slices);
+    smem[i] = ((P.spr * 8 + 15) & ~15) + 4 * nz * P.lpad;
+    slots[i] = slots_for(nz);
+    tmodes[i] = modes[trials[i].point];
+    cost[i] = (double)P.nsteps * (24.0 + 40.0 * P.N * slots[i]);
+    items_by_idx[i] = TrialItem{(int32_t)trials[i].point, (int32_t)i, trials[i].ap};
+  }
+  mcs_plan* pl = new mcs_plan();
+  pl->ctx = c;
+  pl->trials = true;
+  pl->n = n_trials;
+  std::vector<int32_t> order;
+  rc = make_buckets(c, smem, cost, slots, tmodes, true, order, pl->buckets);
+  std::vector<TrialItem> items(n_trials);
+  for (size_t k = 0; k < order.size(); k++) items[k] = items_by_idx[order[k]];
+  const size_t nb = std::max<size_t>(1, pl->buckets.size());
+  if (!rc) rc = pl->params.ensure(sizeof(PointParams) * std::max<size_t>(1, n_points));
+  if (!rc) rc = pl->items.ensure(sizeof(TrialItem) * std::max<size_t>(1, n_trials));
+  if (!rc) rc = pl->results.ensure(sizeof(mcs_trial_result) * std::max<size_t>(1, n_trials));
+  if (!rc) rc = pl->queues.ensure(sizeof(unsigned int) * nb);
+  if (!rc) rc = pl->order.ensure(sizeof(int32_t));
+  cudaError_t e = cudaSuccess;
+  if (!rc && n_trials)
+    rc = upload2(c, c->stream, pl->params.p, pp.data(), sizeof(PointParams) * n_points,
+                 pl->items.p, items.data(), sizeof(TrialItem) * n_trials);
+  if (!rc) rc = enqueue(pl, c->stream, o, nullptr, nullptr, o->chatter_idx);
+  if (!rc && n_trials) {
+    e = cudaMemcpyAsync(out, pl->results.p, sizeof(mcs_trial_result) * n_trials,
+                        cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "result copy failed: %s", cudaGetErrorString(e));
+  }
+  e = cudaStreamSynchronize(c->stream);
+  if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "trials failed: %s", cudaGetErrorString(e));
+  plan_free(pl);
+  return rc;
+}
+
+int mcs_solve_async(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
+                    const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                    size_t n_points, const mcs_opts* opts, mcs_result* out, mcs_job** job) {
+  if (!c || !job) return fail(MCS_ERR_ARG, "NULL ctx or job pointer");
+  if (n_points && !out) return fail(MCS_ERR_ARG, "out is NULL");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  *job = nullptr;
+  mcs_job* jb = new mcs_job();
+  jb->out = out;
+  auto bail = [&](int code) {
+    if (jb->plan) plan_free(jb->plan);
+    jb->cancel.release();
+    jb->progress.release();
+    if (jb->staging) cudaFreeHost(jb->staging);
+    if (jb->done) cudaEventDestroy(jb->done);
+    if (jb->stream) cudaStreamDestroy(jb->stream);
+    delete jb;
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&jb->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&jb->done, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(MCS_ERR_CUDA, "job stream/event creation failed"));
+  int rc = build_plan(c, setups, n_setups, modals, n_modals, points, n_points, opts, false,
+                      jb->stream, &jb->plan);
+  if (rc) return bail(rc);
+  if ((rc = jb->cancel.ensure(sizeof(int))) || (rc = jb->progress.ensure(sizeof(unsigned int))))
+    return bail(rc);
+  if (cudaHostAlloc((void**)&jb->staging, sizeof(mcs_result) * std::max<size_t>(1, n_points),
+                    cudaHostAllocDefault) != cudaSuccess)
+    return bail(fail(MCS_ERR_NOMEM, "pinned staging allocation failed"));
+  if (cudaMemsetAsync(jb->cancel.p, 0, sizeof(int), jb->stream) != cudaSuccess)
+    return bail(fail(MCS_ERR_CUDA, "memset failed"));
+  rc = enqueue(jb->plan, jb->stream, opts, static_cast<const volatile int*>(jb->cancel.p),
+               static_cast<unsigned int*>(jb->progress.p), opts->chatter_idx);
+  if (rc) return bail(rc);
+  if (n_points &&
+      cudaMemcpyAsync(jb->staging, jb->plan->results.p, sizeof(mcs_result) * n_points,
+                      cudaMemcpyDeviceToHost, jb->stream) != cudaSuccess)
+    return bail(fail(MCS_ERR_CUDA, "result copy failed"));
+  if (cudaEventRecord(jb->done, jb->stream) != cudaSuccess)
+    return bail(fail(MCS_ERR_CUDA, "event record failed"));
+  *job = jb;
+  return MCS_OK;
+}
+
+int mcs_job_poll(mcs_job* jb, size_t* points_done, int* finished) {
+  if (!jb) return fail(MCS_ERR_ARG, "job is NULL");
+  mcs_ctx* c = jb->plan->ctx;
+  MCS_CUDA(cudaSetDevice(c->device));
+  const cudaError_t q = cudaEventQuery(jb->done);
+  if (q != cudaSuccess && q != cudaErrorNotReady)
+    return fail(MCS_ERR_CUDA, "job failed: %s", cudaGetErrorString(q));
+  if (finished) *finished = q == cudaSuccess ? 1 : 0;
+  if (points_done) {
+    if (q == cudaSuccess) {
+      *points_done = jb->plan->n;
+    } else {
+      unsigned int v = 0;
+      MCS_CUDA(cudaMemcpyAsync(&v, jb->progress.p, sizeof(v), cudaMemcpyDeviceToHost, c->side));
+      MCS_CUDA(cudaStreamSynchronize(c->side));
+      *points_done = v;
+    }
+  }
+  return MCS_OK;
+}
+
+int mcs_job_cancel(mcs_job* jb) {
+  if (!jb) return fail(MCS_ERR_ARG, "job is NULL");
+  mcs_ctx* c = jb->plan->ctx;
+  MCS_CUDA(cudaSetDevice(c->device));
+  static const int one = 1;
+  MCS_CUDA(cudaMemcpyAsync(jb->cancel.p, &one, sizeof(int), cudaMemcpyHostToDevice, c->side));
+  MCS_CUDA(cudaStreamSynchronize(c->side));
+  return MCS_OK;
+}
+
+int mcs_job_wait(mcs_job* jb) {
+  if (!jb) return fail(MCS_ERR_ARG, "job is NULL");
+  MCS_CUDA(cudaSetDevice(jb->plan->ctx->device));
+  MCS_CUDA(cudaEventSynchronize(jb->done));
+  if (!jb->waited && jb->plan->n) std::memcpy(jb->out, jb->staging, sizeof(mcs_result) * jb->plan->n);
+  jb->waited = true;
+  for (size_t i = 0; i < jb->plan->n; i++)
+    if (jb->out[i].status == MCS_ERR_CANCELLED)
+      return fail(MCS_ERR_CANCELLED, "job was cancelled; %zu points have results", i);
+  return MCS_OK;
+}
+
+void mcs_job_free(mcs_job* jb) {
+  if (!jb) return;
+  cudaSetDevice(jb->plan->ctx->device);
+  cudaEventSynchronize(jb->done);
+  plan_free(jb->plan);
+  jb->cancel.release();
+  jb->progress.release();
+  if (jb->staging) cudaFreeHost(jb->staging);
+  cudaEventDestroy(jb->done);
+  cudaStreamDestroy(jb->stream);
+  delete jb;
+}
+
+int mcs_lobes_alim(mcs_ctx* c, const mcs_modal* modals, size_t n_modals,
+                   const mcs_lobe_query* queries, size_t n_queries, const double* rpm,
+                   size_t n_rpm, double* alim) {
+  if (!c) return fail(MCS_ERR_ARG, "ctx is NULL");
+  if (n_queries && n_rpm && (!modals || !queries || !rpm || !alim))
+    return fail(MCS_ERR_ARG, "NULL input or output array");
+  if (n_queries > 65535 * 64 || n_rpm > (size_t)std::numeric_limits<int32_t>::max())
+    return fail(MCS_ERR_ARG, "too many queries or speeds");
+  int rc = MCS_OK;
+  for (size_t i = 0; i < n_modals; i++) {
+    const mcs_modal& md = modals[i];
+    if (md.nx < 1 || md.nx > kMaxModes || md.ny < 0 || md.ny > kMaxModes)
+      return fail(MCS_ERR_ARG, "modal %zu: 1 <= nx <= %d and 0 <= ny <= %d", i, kMaxModes,
+                  kMaxModes);
+    for (int a = 0; a < 2; a++) {
+      const int cnt = a == 0 ? md.nx : md.ny;
+      const mcs_mode* ms = a == 0 ? md.x : md.y;
+      for (int j = 0; j < cnt; j++)
+        if (!(is_finite(ms[j].k) && ms[j].k > 0 && is_finite(ms[j].fn) && ms[j].fn > 0 &&
+              is_finite(ms[j].zeta) && ms[j].zeta >= 0))
+          return fail(MCS_ERR_ARG, "modal %zu: mode %d needs k > 0, fn > 0, zeta >= 0", i, j);
+    }
+  }
+  for (size_t i = 0; i < n_queries; i++) {
+    const mcs_lobe_query& q = queries[i];
+    if (q.N < 1 || q.lobes < 0 || q.lobes > 10000 || q.modal >= n_modals ||
+        !(is_finite(q.Ktc) && q.Ktc != 0 && is_finite(q.Krc) && is_finite(q.phi_st) &&
+          is_finite(q.phi_ex) && is_finite(q.rpm_min) && is_finite(q.rpm_max)))
+      return fail(MCS_ERR_ARG, "lobe query %zu is invalid", i);
+  }
+  for (size_t r = 0; r < n_rpm; r++)
+    if (!is_finite(rpm[r])) return fail(MCS_ERR_ARG, "rpm %zu is not finite", r);
+  if (!n_queries || !n_rpm) return MCS_OK;
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  DevBuf dm, dq, dr, dout;
+  if ((rc = dm.ensure(sizeof(mcs_modal) * n_modals)) || (rc = dq.ensure(sizeof(mcs_lobe_query) * n_queries)) ||
+      (rc = dr.ensure(sizeof(double) * n_rpm)) || (rc = dout.ensure(sizeof(double) * n_queries * n_rpm))) {
+    dm.release(); dq.release(); dr.release(); dout.release();
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(dm.p, modals, sizeof(mcs_modal) * n_modals, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dq.p, queries, sizeof(mcs_lobe_query) * n_queries, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dr.p, rpm, sizeof(double) * n_rpm, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = (cudaError_t)launch_lobes(c->stream, static_cast<const mcs_modal*>(dm.p),
+                                  static_cast<const mcs_lobe_query*>(dq.p), (int)n_queries,
+                                  static_cast<const double*>(dr.p), (int)n_rpm,
+                                  static_cast<double*>(dout.p));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(alim, dout.p, sizeof(double) * n_queries * n_rpm, cudaMemcpyDeviceToHost, c->stream);
+  cudaError_t e2 = cudaStreamSynchronize(c->stream);
+  dm.release(); dq.release(); dr.release(); dout.release();
+  if (e != cudaSuccess) return fail(MCS_ERR_CUDA, "lobes failed: %s", cudaGetErrorString(e));
+  if (e2 != cudaSuccess) return fail(MCS_ERR_CUDA, "lobes failed: %s", cudaGetErrorString(e2));
+  return MCS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// Internal types shared by the host preparation (mcs_api.cu) and the sm_100a kernels
+// (mcs_kernels.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/mcs.h"
+
+namespace mcs {
+
+constexpr int kMaxTeeth = MCS_MAX_TEETH;
+constexpr int kMaxModes = MCS_MAX_MODES;
+constexpr int kMaxSlots = 2;          // slices per lane: nz <= 64
+constexpr int kWarp = 32;
+constexpr int kMaxSmemPerWarp = 227 * 1024;
+
+// Per-point constants, derived on the host in FP64 exactly as CuttingEngine.configure
+// derives them (src/cutting.js:39-82), plus the engagement window of the static arc map
+// chatterAt builds (src/stabtd.js:17).  One record per (setup, speed, modal) point.
+struct alignas(16) PointParams {
+  double omega;      // spindle angular speed [rad/s]
+  double dphi;       // rotation per step [rad]
+  double R, tanB;    // radius [mm], tan(helix)
+  double flute_len;  // [mm] (chatterAt raises it to ap + 1 per trial)
+  double Ci;         // process-damping coefficient [N/m], 0 when linear
+  double phi_lo;     // engaged angles [phi_lo, phi_hi): bins b0..b1 of the arc map
+  double phi_hi;
+  float fz, hmax;    // feed per tooth, chip-thickness cap [mm]
+  float Ktc, Krc, Kte, Kre;
+  float mc;          // size-effect exponent, 0 when linear
+  float dtf;         // step [s]
+  float dR[kMaxTeeth];                  // runout offset of each tooth [mm]
+  float mk[2][kMaxModes];               // modal stiffness [N/m] (x, y)
+  float mcd[2][kMaxModes];              // modal damping [N s/m]
+  float ma[2][kMaxModes];               // dt / modal mass
+  int32_t N, spt, spr, decim;
+  int32_t nsteps;                       // spt * N * revs
+  int32_t type;                         // mcs_tool_type
+  int32_t slices_override;              // > 0: equal slices
+  int32_t excl_zero;                    // arc map starts at bin 0: phi == 0 is not in cut
+  int32_t lpad;                         // ring row pitch (floats)
+  int32_t nz_max;                       // slices at the deepest trial of the point
+  int32_t ts_c0;                        // first tooth sample inside the index window
+  int32_t ts_n;                         // tooth samples in the window (<= 24)
+  int32_t hist_h0;                      // first history sample inside the window
+  int32_t hist_m;                       // history samples in the window
+  int32_t smem_bytes;                   // table + ring for the deepest trial
+  int32_t empty;                        // arc covers no bin
+};
+
+// Options the kernels read (mcs_opts reduced to what the device needs).
+struct DevOpts {
+  double a_min, a_max, chatter_idx;
+  int32_t iters, pad;
+};
+
+// One chatterAt trial of the batch kernel.
+struct TrialItem {
+  int32_t point;   // index into the PointParams array
+  int32_t out;     // index into the caller's result array
+  double ap;
+};
+
+// Launch shapes (template parameters) the kernels are instantiated for.
+struct KernelShape {
+  int slots;  // 1 or 2
+  int modes;  // 1..4
+};
+
+// Host launchers (mcs_kernels.cu).
+int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
+                 const PointParams* pts, const int32_t* order, int n, DevOpts opts,
+                 mcs_result* out, unsigned int* queue, const volatile int* cancel,
+                 unsigned int* progress);
+int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
+                  const PointParams* pts, const TrialItem* items, int n, double chatter_idx,
+                  mcs_trial_result* out, unsigned int* queue);
+int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm);
+int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm);
+int set_smem_limits();
+int launch_lobes(cudaStream_t stream, const mcs_modal* modals, const mcs_lobe_query* qs, int n_q,
+                 const double* rpm, int n_rpm, double* out);
+
+}  // namespace mcs

@@ -1,0 +1,24 @@
+"""mcs -- B200 time-domain chatter stability (host layer over libmcs.so).
+
+The functions mirror the reference's JavaScript API for this path:
+
+  timeDomainLimit, chatterAt          src/stabtd.js:14-32
+  timeDomainLimits (the Worker sweep) src/stabworker.js:6-14
+  StabWorker (the message protocol)   src/stabworker.js:1-15
+  lobeLimit (stabilityLobes + alimAt) src/sld.js:23-76
+
+All compute runs in the CUDA library; a missing library or device raises.
+"""
+from ._abi import (CHATTER_IDX, DEFAULTS, make_material, make_modal, make_opts, make_setup,
+                   make_tool)
+from ._lib import Context, Job, MCSError, Plan, default_context, load
+from .sld import lobeLimit, lobeLimits
+from .stabtd import chatterAt, chatterIndex, timeDomainLimit, timeDomainLimits
+from .worker import StabWorker
+
+__all__ = [
+    "CHATTER_IDX", "DEFAULTS", "Context", "Job", "MCSError", "Plan", "StabWorker",
+    "chatterAt", "chatterIndex", "default_context", "load", "lobeLimit", "lobeLimits",
+    "make_material", "make_modal", "make_opts", "make_setup", "make_tool", "timeDomainLimit",
+    "timeDomainLimits",
+]

@@ -1,0 +1,260 @@
+"""ctypes binding of libmcs.so (include/mcs.h) and the Context that owns a device.
+
+The library is the only compute path: if libmcs.so is missing or no CUDA device is
+present, every call raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+from typing import Sequence
+
+import numpy as np
+
+from . import _abi as A
+
+PKG = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG / "libmcs.so"
+
+# every symbol include/mcs.h declares
+EXPORTS = (
+    "mcs_default_opts", "mcs_last_error", "mcs_create", "mcs_destroy", "mcs_stream",
+    "mcs_solve", "mcs_chatter_at", "mcs_plan_create", "mcs_plan_execute", "mcs_plan_results",
+    "mcs_plan_info_get", "mcs_plan_destroy", "mcs_solve_async", "mcs_job_poll",
+    "mcs_job_cancel", "mcs_job_wait", "mcs_job_free", "mcs_lobes_alim",
+)
+
+_LIB = None
+_LOCK = threading.Lock()
+
+
+class MCSError(RuntimeError):
+    """A non-OK mcs_status, with mcs_last_error()'s message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{A.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def load(path: Path | str | None = None):
+    """Load libmcs.so and declare its prototypes (raises if it is not built)."""
+    global _LIB
+    with _LOCK:
+        if _LIB is not None and path is None:
+            return _LIB
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise ImportError(f"{p} is not built: run `python machinig-sim_b200/build.py`")
+        L = C.CDLL(str(p))
+        P = C.POINTER
+        vp = C.c_void_p
+        L.mcs_default_opts.argtypes = [P(A.Opts)]
+        L.mcs_default_opts.restype = None
+        L.mcs_last_error.restype = C.c_char_p
+        L.mcs_create.argtypes = [P(vp), C.c_int]
+        L.mcs_destroy.argtypes = [vp]
+        L.mcs_stream.argtypes = [vp]
+        L.mcs_stream.restype = vp
+        batch = [vp, vp, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, P(A.Opts)]
+        L.mcs_solve.argtypes = batch + [vp]
+        L.mcs_chatter_at.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, vp,
+                                     C.c_size_t, P(A.Opts), vp]
+        L.mcs_plan_create.argtypes = batch + [P(vp)]
+        L.mcs_plan_execute.argtypes = [vp]
+        L.mcs_plan_results.argtypes = [vp, vp]
+        L.mcs_plan_info_get.argtypes = [vp, P(A.PlanInfo)]
+        L.mcs_plan_destroy.argtypes = [vp]
+        L.mcs_solve_async.argtypes = batch + [vp, P(vp)]
+        L.mcs_job_poll.argtypes = [vp, P(C.c_size_t), P(C.c_int)]
+        L.mcs_job_cancel.argtypes = [vp]
+        L.mcs_job_wait.argtypes = [vp]
+        L.mcs_job_free.argtypes = [vp]
+        L.mcs_job_free.restype = None
+        L.mcs_lobes_alim.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, vp]
+        for name in EXPORTS:
+            if name not in ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free"):
+                getattr(L, name).restype = C.c_int
+        if path is None:
+            _LIB = L
+        return L
+
+
+def last_error() -> str:
+    return (load().mcs_last_error() or b"").decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != A.MCS_OK:
+        raise MCSError(status, last_error())
+
+
+def default_opts() -> A.Opts:
+    o = A.Opts()
+    load().mcs_default_opts(C.byref(o))
+    return o
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data) if a.size else C.c_void_p(0)
+
+
+class Batch:
+    """Inputs of a solve as contiguous record arrays (setups, modals, points)."""
+
+    def __init__(self, setups, modals, points):
+        self.setups = A.as_records(setups, A.SETUP_DTYPE)
+        self.modals = A.as_records(modals, A.MODAL_DTYPE)
+        self.points = A.as_records(points, A.POINT_DTYPE)
+
+    def args(self):
+        return (_ptr(self.setups), len(self.setups), _ptr(self.modals), len(self.modals),
+                _ptr(self.points), len(self.points))
+
+
+class Plan:
+    """Device-resident solve batch launched as a captured CUDA graph."""
+
+    def __init__(self, ctx: "Context", batch: Batch, opts: A.Opts):
+        self.ctx = ctx
+        self.batch = batch
+        self.n = len(batch.points)
+        h = C.c_void_p()
+        check(ctx._L.mcs_plan_create(ctx._h, *batch.args(), C.byref(opts), C.byref(h)))
+        self._h = h
+
+    def execute(self) -> None:
+        check(self.ctx._L.mcs_plan_execute(self._h))
+
+    def results(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=A.RESULT_DTYPE)
+        check(self.ctx._L.mcs_plan_results(self._h, _ptr(out)))
+        return out
+
+    def info(self) -> dict:
+        i = A.PlanInfo()
+        check(self.ctx._L.mcs_plan_info_get(self._h, C.byref(i)))
+        return {n: getattr(i, n) for n, _ in A.PlanInfo._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.ctx._L.mcs_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Job:
+    """Asynchronous solve (the Worker protocol): poll, cancel, wait."""
+
+    def __init__(self, ctx: "Context", batch: Batch, opts: A.Opts):
+        self.ctx = ctx
+        self.batch = batch
+        self.n = len(batch.points)
+        self.out = np.zeros(max(1, self.n), dtype=A.RESULT_DTYPE)
+        h = C.c_void_p()
+        check(ctx._L.mcs_solve_async(ctx._h, *batch.args(), C.byref(opts), _ptr(self.out),
+                                     C.byref(h)))
+        self._h = h
+
+    def poll(self) -> tuple[int, bool]:
+        done = C.c_size_t()
+        fin = C.c_int()
+        check(self.ctx._L.mcs_job_poll(self._h, C.byref(done), C.byref(fin)))
+        return int(done.value), bool(fin.value)
+
+    def cancel(self) -> None:
+        check(self.ctx._L.mcs_job_cancel(self._h))
+
+    def wait(self) -> np.ndarray:
+        """Results; raises MCSError(MCS_ERR_CANCELLED) after a cancel (results still set)."""
+        st = self.ctx._L.mcs_job_wait(self._h)
+        if st not in (A.MCS_OK, A.MCS_ERR_CANCELLED):
+            check(st)
+        self.cancelled = st == A.MCS_ERR_CANCELLED
+        return self.out[: self.n]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.ctx._L.mcs_job_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """One CUDA device (mcs_create).  Thread-safe: the library serialises calls."""
+
+    def __init__(self, device: int = 0):
+        self._L = load()
+        h = C.c_void_p()
+        check(self._L.mcs_create(C.byref(h), int(device)))
+        self._h = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.mcs_stream(self._h) or 0)
+
+    def solve(self, setups, modals, points, opts: A.Opts) -> np.ndarray:
+        b = Batch(setups, modals, points)
+        out = np.zeros(max(1, len(b.points)), dtype=A.RESULT_DTYPE)
+        check(self._L.mcs_solve(self._h, *b.args(), C.byref(opts), _ptr(out)))
+        return out[: len(b.points)]
+
+    def chatter_at(self, setups, modals, points, trials, opts: A.Opts) -> np.ndarray:
+        b = Batch(setups, modals, points)
+        t = A.as_records(trials, A.TRIAL_DTYPE)
+        out = np.zeros(max(1, len(t)), dtype=A.TRIAL_RESULT_DTYPE)
+        check(self._L.mcs_chatter_at(self._h, *b.args(), _ptr(t), len(t), C.byref(opts),
+                                     _ptr(out)))
+        return out[: len(t)]
+
+    def plan(self, setups, modals, points, opts: A.Opts) -> Plan:
+        return Plan(self, Batch(setups, modals, points), opts)
+
+    def solve_async(self, setups, modals, points, opts: A.Opts) -> Job:
+        return Job(self, Batch(setups, modals, points), opts)
+
+    def lobes_alim(self, modals, queries: Sequence[A.LobeQuery], rpm) -> np.ndarray:
+        m = A.as_records(modals, A.MODAL_DTYPE)
+        q = A.array_of(A.LobeQuery, list(queries))
+        r = np.ascontiguousarray(rpm, dtype=np.float64)
+        out = np.zeros((len(queries), len(r)), dtype=np.float64)
+        check(self._L.mcs_lobes_alim(self._h, _ptr(m), len(m), C.cast(q, C.c_void_p),
+                                     len(queries), _ptr(r), len(r), _ptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.mcs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_DEFAULT: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    """A process-wide context per device, created on first use."""
+    with _LOCK:
+        ctx = _DEFAULT.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        with _LOCK:
+            _DEFAULT.setdefault(device, ctx)
+            ctx = _DEFAULT[device]
+    return ctx
