@@ -200,12 +200,11 @@ def ours(args) -> int:
     from mcs import workloads as W
 
     wl = W.sweep(seed=1 + rank)
+    if args.points and args.points < wl.n:  # a smaller case of the same sweep (profiling)
+        wl = wl.subset(np.linspace(0, wl.n - 1, args.points).round().astype(int))
     ctx = mcs.Context(device)
     stream = torch.cuda.ExternalStream(ctx.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
-
-    plan = ctx.plan(wl.setups, wl.modals, wl.points, wl.opts)
-    info = plan.info()
 
     def barrier():
         if dist is not None:
@@ -218,28 +217,47 @@ def ours(args) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):
-        plan.execute()
-    res = plan.results()
-    assert np.all(res["status"] == 0), np.unique(res["status"])
-
-    # ---- value: device-resident inputs, CUDA events on the launching stream ----
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(device) as clk:
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(i & 0xFF)  # write 256 MiB (> 126 MB L2) between timed steps
-            starts[i].record(stream)
+    def timed(precision: str):
+        """Device-resident plan of the sweep: per-step CUDA-event times, results, info."""
+        opts = A.make_opts(precision=precision)
+        for f in ("a_min", "a_max", "iters", "revs", "nonlinear", "honor_runout",
+                  "steps_per_tooth", "slices", "chatter_idx"):
+            setattr(opts, f, getattr(wl.opts, f))
+        plan = ctx.plan(wl.setups, wl.modals, wl.points, opts)
+        info = plan.info()
+        for _ in range(args.warmup):
             plan.execute()
-            ends[i].record(stream)
+        res = plan.results()
+        assert np.all((res["status"] == 0) | (res["status"] == 4)), np.unique(res["status"])
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        barrier()
         torch.cuda.synchronize()
-    barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    ms = maxover(float(np.sum(step_ms))) / args.steps
-    res = plan.results()
+        with ClockSampler(device) as clk:
+            for i in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(i & 0xFF)  # write 256 MiB (> 126 MB L2) between timed steps
+                starts[i].record(stream)
+                plan.execute()
+                ends[i].record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
+        res = plan.results()
+        plan.close()
+        return step_ms, res, info, clk.summary(), opts
+
+    from mcs import _abi as A
+
+    variants = {}
+    for prec in (["fp32", "fp64"] if not args.fp32_only else [args.precision]):
+        step_ms, res, info, clocks, opts = timed(prec)
+        ms = maxover(float(np.sum(step_ms))) / args.steps
+        variants[prec] = {"step_ms": step_ms, "ms": ms, "res": res, "info": info,
+                          "clocks": clocks, "opts": opts}
+    main = variants[args.precision]
+    step_ms, ms, res, info, clocks = (main["step_ms"], main["ms"], main["res"], main["info"],
+                                      main["clocks"])
     pts_total = wl.n * world
     value = pts_total / (ms / 1e3)
 
@@ -249,44 +267,47 @@ def ours(args) -> int:
     engaged = float(res["engaged"].sum())
     flop = FLOP_ENGAGED * engaged + FLOP_IDLE * (evals - engaged)
     achieved_tflops = flop / (float(np.mean(step_ms)) / 1e3) / 1e12
-    clocks = clk.summary()
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     f_mhz = clocks["sm_mhz"] or 1965.0
     peak_tflops = sms * 128 * 2 * f_mhz * 1e6 / 1e12
 
     # ---- e2e: public blocking API from page-locked host buffers ----
+    e2e = None
     def pinned(arr):
         t = torch.empty(arr.nbytes, dtype=torch.uint8, pin_memory=True)
         v = t.numpy().view(arr.dtype)
         v[:] = arr
         return t, v
 
-    keep = []
-    hs = [pinned(wl.setups), pinned(wl.modals), pinned(wl.points)]
-    keep += hs
-    from mcs import _abi as A
-    out_t = torch.empty(len(wl.points) * A.RESULT_DTYPE.itemsize, dtype=torch.uint8,
-                        pin_memory=True)
-    out_v = out_t.numpy().view(A.RESULT_DTYPE)
-    import ctypes as C
+    if not args.no_e2e:
+        keep = []
+        hs = [pinned(wl.setups), pinned(wl.modals), pinned(wl.points)]
+        keep += hs
+        out_t = torch.empty(len(wl.points) * A.RESULT_DTYPE.itemsize, dtype=torch.uint8,
+                            pin_memory=True)
+        out_v = out_t.numpy().view(A.RESULT_DTYPE)
+        import ctypes as C
 
-    L = ctx._L
-    args_c = (ctx._h, C.c_void_p(hs[0][1].ctypes.data), len(wl.setups),
-              C.c_void_p(hs[1][1].ctypes.data), len(wl.modals),
-              C.c_void_p(hs[2][1].ctypes.data), len(wl.points), C.byref(wl.opts),
-              C.c_void_p(out_v.ctypes.data))
-    for _ in range(max(1, args.warmup // 2)):
-        mcs._lib.check(L.mcs_solve(*args_c))
-    e2e_steps = max(2, min(args.steps, 5))
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        mcs._lib.check(L.mcs_solve(*args_c))
-    torch.cuda.synchronize()
-    e2e_s = maxover(time.perf_counter() - t0) / e2e_steps
-    barrier()
-    assert np.array_equal(out_v["alim"], res["alim"]), "e2e and plan results differ"
+        L = ctx._L
+        args_c = (ctx._h, C.c_void_p(hs[0][1].ctypes.data), len(wl.setups),
+                  C.c_void_p(hs[1][1].ctypes.data), len(wl.modals),
+                  C.c_void_p(hs[2][1].ctypes.data), len(wl.points), C.byref(main["opts"]),
+                  C.c_void_p(out_v.ctypes.data))
+        for _ in range(max(1, args.warmup // 2)):
+            mcs._lib.check(L.mcs_solve(*args_c))
+        e2e_steps = max(2, min(args.steps, 5))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            mcs._lib.check(L.mcs_solve(*args_c))
+        torch.cuda.synchronize()
+        e2e_s = maxover(time.perf_counter() - t0) / e2e_steps
+        barrier()
+        assert np.array_equal(out_v["alim"], res["alim"]), "e2e and plan results differ"
+        e2e = {"value": pts_total / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(info["h2d_bytes"]),
+               "d2h_bytes_per_step": int(info["d2h_bytes"])}
 
     line = None
     if rank == 0:
@@ -294,11 +315,14 @@ def ours(args) -> int:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64",
             "data": "synthetic (seeded sweep; no public dataset exists for this path)",
             "config": {"workload": "sweep: 4096 speeds 3000-30000 rpm, 4-flute D10 helix 30, "
                                    "3+3 modes, 10 um runout, [0.05,15] x 10, 60 revs, 40 slices",
-                       "points_per_gpu": wl.n, "variant": "plain GPU bisection",
+                       "points_per_gpu": wl.n,
+                       "variant": f"plain GPU bisection, {args.precision} force law and "
+                                  "modal integration, FP64 statistics and bracket",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "kernels_per_step": info["kernels"], "graph": bool(info["graph"]),
                        "blocks": info["blocks"], "smem_per_warp_max": info["smem_per_warp"]},
@@ -312,15 +336,15 @@ def ours(args) -> int:
                                  f"out-of-cut reference evaluation; {evals:.3e} evaluations, "
                                  f"{engaged:.3e} in cut per step"},
             "cpu_baseline": cpu,
-            "e2e": {"value": pts_total / e2e_s, "unit": UNIT,
-                    "h2d_bytes_per_step": int(info["h2d_bytes"]),
-                    "d2h_bytes_per_step": int(info["d2h_bytes"])},
+            "e2e": e2e,
             "gpu_launches": int(info["kernels"]) * args.steps,
             "clocks": clocks,
             "results": {"open": int(res["open"].sum()), "alim_median": float(np.median(res["alim"]))},
+            "variants": {k: {"value": pts_total / (v["ms"] / 1e3), "ms_per_step": v["ms"],
+                             "kernels_per_step": v["info"]["kernels"],
+                             "sm_mhz": v["clocks"]["sm_mhz"]} for k, v in variants.items()},
         }
         print(json.dumps(line), flush=True)
-    plan.close()
     ctx.close()
     if dist is not None:
         dist.barrier()
@@ -335,6 +359,12 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
+                    help="integration precision of the headline value")
+    ap.add_argument("--fp32-only", action="store_true", help="time only the headline precision")
+    ap.add_argument("--points", type=int, default=0,
+                    help="solve an evenly spaced subset of the sweep (profiling case)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         a.warmup = 3

@@ -49,6 +49,11 @@ typedef enum {
 
 typedef enum { MCS_TOOL_FLAT = 0, MCS_TOOL_BALL = 1 } mcs_tool_type;
 
+/* Arithmetic of the per-step force law and modal integration.  The once-per-tooth
+ * statistics, the chatter index and the bisection bracket are FP64 in both; the surface
+ * ring is float in both (the reference's Float32Array). */
+typedef enum { MCS_FP32 = 0, MCS_FP64 = 1 } mcs_precision;
+
 /* One mode of the tool tip: frf.js:1-11 {k [N/mm], fn [Hz], zeta}. */
 typedef struct {
   double k;
@@ -109,6 +114,8 @@ typedef struct {
   int32_t steps_per_tooth; /* 0: reference rule max(48, ceil(Ttooth*fTop*24)) */
   int32_t slices;          /* 0: reference rule dz = max(0.25, fluteLen/48) */
   double chatter_idx;      /* decision threshold (reference 0.45, stabtd.js:10) */
+  int32_t precision;       /* mcs_precision of the force law and modal integration */
+  int32_t pad;
 } mcs_opts;
 
 /* Result of timeDomainLimit for one point. */

@@ -63,6 +63,8 @@ int check_inputs(const mcs_setup* setups, size_t n_setups, const mcs_modal* moda
   if (o->slices > kMaxSlots * kWarp)
     return fail(MCS_ERR_UNSUPPORTED, "at most %d slices are supported", kMaxSlots * kWarp);
   if (!is_finite(o->chatter_idx)) return fail(MCS_ERR_ARG, "chatter_idx is not finite");
+  if (o->precision != MCS_FP32 && o->precision != MCS_FP64)
+    return fail(MCS_ERR_ARG, "precision must be MCS_FP32 or MCS_FP64");
   for (size_t i = 0; i < n_setups; i++) {
     const mcs_setup& s = setups[i];
     const mcs_tool& t = s.tool;
@@ -154,18 +156,17 @@ int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const m
   P.tanB = std::tan(t.helix_deg * kPi / 180);
   P.flute_len = t.flute_len;
   P.Ci = o.nonlinear ? st.mat.Ci : 0.0;
-  P.fz = (float)st.fz;
-  P.hmax = (float)std::max(0.1, 3 * st.fz);
-  P.Ktc = (float)st.mat.Ktc;
-  P.Krc = (float)st.mat.Krc;
-  P.Kte = (float)st.mat.Kte;
-  P.Kre = (float)st.mat.Kre;
-  P.mc = o.nonlinear ? (float)st.mat.mc : 0.f;
-  P.dtf = (float)dt;
+  P.fz = st.fz;
+  P.hmax = std::max(0.1, 3 * st.fz);
+  P.Ktc = st.mat.Ktc;
+  P.Krc = st.mat.Krc;
+  P.Kte = st.mat.Kte;
+  P.Kre = st.mat.Kre;
+  P.mc = o.nonlinear ? st.mat.mc : 0.0;
+  P.dt = dt;
   // runout offsets delta_i = e cos(2 pi i / N - gamma) (cutting.js:44); chatterAt uses 0
   for (int i = 0; i < N; i++)
-    P.dR[i] = o.honor_runout ? (float)(t.runout * std::cos(2 * kPi * i / N - t.runout_phase))
-                             : 0.f;
+    P.dR[i] = o.honor_runout ? t.runout * std::cos(2 * kPi * i / N - t.runout_phase) : 0.0;
   // modes: k [N/m], m = k / (2 pi fn)^2, c = 2 zeta sqrt(k m) (cutting.js:54-59)
   for (int a = 0; a < 2; a++) {
     const int cnt = a == 0 ? nx : ny;
@@ -175,9 +176,9 @@ int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const m
       const double w = 2 * kPi * ms[j].fn;
       const double m = k / (w * w);
       const double c = 2 * ms[j].zeta * std::sqrt(k * m);
-      P.mk[a][j] = (float)k;
-      P.mcd[a][j] = (float)c;
-      P.ma[a][j] = (float)(dt / m);
+      P.mk[a][j] = k;
+      P.mcd[a][j] = c;
+      P.ma[a][j] = dt / m;
     }
   }
   out.modes = std::max(nx, ny);
@@ -222,7 +223,8 @@ int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const m
   const long long H = (long long)P.nsteps / P.decim;
   P.hist_m = (int)std::min<long long>(H, (long long)std::floor((double)P.ts_n * spt / P.decim + 0.5));
   P.hist_h0 = (int)(H - P.hist_m);
-  const long long smem = (long long)((P.spr * 8 + 15) & ~15) + 4LL * P.nz_max * P.lpad;
+  const long long smem = (long long)table_bytes(P.spr, o.precision == MCS_FP64) +
+                         4LL * P.nz_max * P.lpad;
   if (smem > kMaxSmemPerWarp)
     return fail(MCS_ERR_UNSUPPORTED,
                 "point needs %lld bytes of shared memory (spr %d, %d slices): above %d", smem,
@@ -317,7 +319,7 @@ namespace {
 // shared-memory need, each launched as its own persistent grid.
 int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
                  const std::vector<int>& slots, const std::vector<int>& modes, bool trials,
-                 std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
+                 int fp64, std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
   const size_t n = smem.size();
   std::vector<int32_t> idx(n);
   std::iota(idx.begin(), idx.end(), 0);
@@ -351,7 +353,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     b.offset = (int)order.size();
     b.count = (int)seg.size();
     b.smem = (top + 15) & ~15;
-    b.shape = KernelShape{sl, nm};
+    b.shape = KernelShape{sl, nm, fp64};
     order.insert(order.end(), seg.begin(), seg.end());
     int bps = 0;
     const int rc = trials ? occupancy_trials(b.shape, b.smem, &bps)
@@ -478,7 +480,8 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
-  rc = make_buckets(ctx, smem, cost, slots, modes, false, order, pl->buckets);
+  rc = make_buckets(ctx, smem, cost, slots, modes, false, o->precision == MCS_FP64, order,
+                    pl->buckets);
   if (rc) {
     plan_free(pl);
     return rc;
@@ -543,6 +546,8 @@ void mcs_default_opts(mcs_opts* o) {
   o->steps_per_tooth = 0;
   o->slices = 0;
   o->chatter_idx = 0.45;
+  o->precision = MCS_FP32;
+  o->pad = 0;
 }
 
 const char* mcs_last_error(void) { return g_last_error.c_str(); }
@@ -726,7 +731,7 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
   for (size_t i = 0; i < n_trials; i++) {
     const PointParams& P = pp[trials[i].point];
     const int nz = slices_at(trials[i].ap, P.flute_len, o->slices);
-    smem[i] = ((P.spr * 8 + 15) & ~15) + 4 * nz * P.lpad;
+    smem[i] = table_bytes(P.spr, o->precision == MCS_FP64) + 4 * nz * P.lpad;
     slots[i] = slots_for(nz);
     tmodes[i] = modes[trials[i].point];
     cost[i] = (double)P.nsteps * (24.0 + 40.0 * P.N * slots[i]);
@@ -737,7 +742,8 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
   pl->trials = true;
   pl->n = n_trials;
   std::vector<int32_t> order;
-  rc = make_buckets(c, smem, cost, slots, tmodes, true, order, pl->buckets);
+  rc = make_buckets(c, smem, cost, slots, tmodes, true, o->precision == MCS_FP64, order,
+                    pl->buckets);
   std::vector<TrialItem> items(n_trials);
   for (size_t k = 0; k < order.size(); k++) items[k] = items_by_idx[order[k]];
   const size_t nb = std::max<size_t>(1, pl->buckets.size());

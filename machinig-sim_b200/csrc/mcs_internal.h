@@ -20,19 +20,19 @@ constexpr int kMaxSmemPerWarp = 227 * 1024;
 struct alignas(16) PointParams {
   double omega;      // spindle angular speed [rad/s]
   double dphi;       // rotation per step [rad]
+  double dt;         // step [s]
   double R, tanB;    // radius [mm], tan(helix)
   double flute_len;  // [mm] (chatterAt raises it to ap + 1 per trial)
   double Ci;         // process-damping coefficient [N/m], 0 when linear
   double phi_lo;     // engaged angles [phi_lo, phi_hi): bins b0..b1 of the arc map
   double phi_hi;
-  float fz, hmax;    // feed per tooth, chip-thickness cap [mm]
-  float Ktc, Krc, Kte, Kre;
-  float mc;          // size-effect exponent, 0 when linear
-  float dtf;         // step [s]
-  float dR[kMaxTeeth];                  // runout offset of each tooth [mm]
-  float mk[2][kMaxModes];               // modal stiffness [N/m] (x, y)
-  float mcd[2][kMaxModes];              // modal damping [N s/m]
-  float ma[2][kMaxModes];               // dt / modal mass
+  double fz, hmax;   // feed per tooth, chip-thickness cap [mm]
+  double Ktc, Krc, Kte, Kre;
+  double mc;         // size-effect exponent, 0 when linear
+  double dR[kMaxTeeth];                 // runout offset of each tooth [mm]
+  double mk[2][kMaxModes];              // modal stiffness [N/m] (x, y); 0 when padded
+  double mcd[2][kMaxModes];             // modal damping [N s/m]
+  double ma[2][kMaxModes];              // dt / modal mass
   int32_t N, spt, spr, decim;
   int32_t nsteps;                       // spt * N * revs
   int32_t type;                         // mcs_tool_type
@@ -47,6 +47,13 @@ struct alignas(16) PointParams {
   int32_t smem_bytes;                   // table + ring for the deepest trial
   int32_t empty;                        // arc covers no bin
 };
+
+// Shared memory of one warp: the sin/cos table of the revolution's positions (float2 or
+// double2 by integration precision) followed by the surface ring (always float: the
+// reference stores the surface in a Float32Array).
+__host__ __device__ inline int table_bytes(int spr, bool fp64) {
+  return (spr * (fp64 ? 16 : 8) + 15) & ~15;
+}
 
 // Options the kernels read (mcs_opts reduced to what the device needs).
 struct DevOpts {
@@ -65,6 +72,7 @@ struct TrialItem {
 struct KernelShape {
   int slots;  // 1 or 2
   int modes;  // 1..4
+  int fp64;   // 0: FP32 force law and modal integration, 1: FP64
 };
 
 // Host launchers (mcs_kernels.cu).

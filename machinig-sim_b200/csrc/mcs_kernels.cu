@@ -9,7 +9,8 @@
 //     geometry (cutting.js:98-124) lives in registers for the whole trial;
 //   * per step the N teeth are visited in turn; a tooth whose slices are all outside
 //     the engaged arc is skipped by the whole warp (vote), otherwise every lane whose
-//     slice is in cut evaluates the force law (cutting.js:181-207) in FP32;
+//     slice is in cut evaluates the force law (cutting.js:181-207) in FP32 (or FP64
+//     when the caller asks for it: the kernels are templated on the scalar type);
 //   * Fx, Fy are summed with a butterfly of shuffles, so every lane holds the total and
 //     runs the modal update (semi-implicit Euler, cutting.js:246-255) redundantly;
 //   * the once-per-tooth samples of the chatter-index window sit one per lane, and the
@@ -50,7 +51,30 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-__host__ __device__ __forceinline__ int table_bytes(int spr) { return (spr * 8 + 15) & ~15; }
+// Arithmetic of the integration scalar T (float or double).
+template <typename T>
+struct Arith;
+template <>
+struct Arith<float> {
+  using V2 = float2;
+  static __device__ __forceinline__ float madd(float a, float b, float c) { return fmaf(a, b, c); }
+  // se * h with se = (H_REF / max(h, H_MIN))^mc (cutting.js:197), MUFU log2/exp2
+  static __device__ __forceinline__ float size_effect(float h, float mc) {
+    return h * exp2f(mc * (kLog2HRef - __log2f(fmaxf(h, kHMin))));
+  }
+  static __device__ __forceinline__ float2 pair(double s, double c) {
+    return make_float2((float)s, (float)c);
+  }
+};
+template <>
+struct Arith<double> {
+  using V2 = double2;
+  static __device__ __forceinline__ double madd(double a, double b, double c) { return fma(a, b, c); }
+  static __device__ __forceinline__ double size_effect(double h, double mc) {
+    return h * pow(0.05 / (h > 0.002 ? h : 0.002), mc);
+  }
+  static __device__ __forceinline__ double2 pair(double s, double c) { return make_double2(s, c); }
+};
 
 struct TrialOut {
   double index, once, amp;
@@ -59,23 +83,25 @@ struct TrialOut {
 };
 
 // sin/cos of every position of one revolution: theta(p) = p * dphi.
-__device__ __forceinline__ void build_table(const PointParams* __restrict__ P, float2* table,
-                                            int lane) {
+template <typename T>
+__device__ __forceinline__ void build_table(const PointParams* __restrict__ P,
+                                            typename Arith<T>::V2* table, int lane) {
   const int spr = P->spr;
   const double dphi = P->dphi;
   for (int p = lane; p < spr; p += kWarp) {
     double s, c;
     sincos(p * dphi, &s, &c);
-    table[p] = make_float2((float)s, (float)c);
+    table[p] = Arith<T>::pair(s, c);
   }
   __syncwarp();
 }
 
 // One chatterAt trial at depth ap: configure + setEngagement + kick + run + chatterIndex.
-template <int SLOTS, int NM>
+template <typename T, int SLOTS, int NM>
 __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
-                                   const float2* __restrict__ table, float* __restrict__ ring,
-                                   int lane) {
+                                   const typename Arith<T>::V2* __restrict__ table,
+                                   float* __restrict__ ring, int lane) {
+  using A = Arith<T>;
   TrialOut res;
   const int N = P->N, spt = P->spt, spr = P->spr, lpad = P->lpad;
 
@@ -94,13 +120,13 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   // process damping per slice, Ci*b/V_c (cutting.js:155-156,203)
   const double pdK = P->Ci != 0.0 ? P->Ci * dz * 1e-3 / (P->omega * 1e-3) : 0.0;
 
-  float sL[SLOTS], cL[SLOTS], ktb[SLOTS], kteb[SLOTS], krb[SLOTS], kreb[SLOTS], pdc[SLOTS],
+  T sL[SLOTS], cL[SLOTS], ktb[SLOTS], kteb[SLOTS], krb[SLOTS], kreb[SLOTS], pdc[SLOTS],
       fzk[SLOTS];
   int p0[SLOTS], len[SLOTS], base[SLOTS];
 #pragma unroll
   for (int s = 0; s < SLOTS; s++) {
     const int k = lane + kWarp * s;
-    sL[s] = cL[s] = ktb[s] = kteb[s] = krb[s] = kreb[s] = pdc[s] = fzk[s] = 0.f;
+    sL[s] = cL[s] = ktb[s] = kteb[s] = krb[s] = kreb[s] = pdc[s] = fzk[s] = T(0);
     p0[s] = 0;
     len[s] = 0;
     base[s] = k * lpad;
@@ -116,8 +142,8 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
       const double lag = zr * P->tanB / P->R;
       double sl, cl;
       sincos(lag, &sl, &cl);
-      sL[s] = (float)sl;
-      cL[s] = (float)cl;
+      sL[s] = (T)sl;
+      cL[s] = (T)cl;
       // positions p whose angle p*dphi - lag (mod 2pi) falls in [phi_lo, phi_hi)
       const double u = (P->phi_lo + lag) / P->dphi;
       const double w = (P->phi_hi + lag) / P->dphi;
@@ -131,38 +157,38 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
       if (pc < 0) pc += spr;
       p0[s] = (int)pc;
       len[s] = (int)fmin(fmax(L, 0.0), (double)lpad);
-      ktb[s] = (float)(P->Ktc * b);
-      kteb[s] = (float)(P->Kte * b);
-      krb[s] = (float)(P->Krc * b);
-      kreb[s] = (float)(P->Kre * b);
-      pdc[s] = (float)(pdK * (b / dz) / r);
-      fzk[s] = (float)((double)P->fz * kap);
+      ktb[s] = (T)(P->Ktc * b);
+      kteb[s] = (T)(P->Kte * b);
+      krb[s] = (T)(P->Krc * b);
+      kreb[s] = (T)(P->Kre * b);
+      pdc[s] = (T)(pdK * (b / dz) / r);
+      fzk[s] = (T)(P->fz * kap);
     }
   }
   // a fresh engine's surface is all zeros (cutting.js:68)
   for (int i = lane; i < nz * lpad; i += kWarp) ring[i] = 0.f;
   __syncwarp();
 
-  float dRr[kMaxTeeth];
+  T dRr[kMaxTeeth];
 #pragma unroll
-  for (int i = 0; i < kMaxTeeth; i++) dRr[i] = P->dR[i];
-  float mk[2][NM], mcd[2][NM], ma[2][NM], q[2][NM], v[2][NM];
+  for (int i = 0; i < kMaxTeeth; i++) dRr[i] = (T)P->dR[i];
+  T mk[2][NM], mcd[2][NM], ma[2][NM], q[2][NM], v[2][NM];
 #pragma unroll
   for (int a = 0; a < 2; a++)
 #pragma unroll
     for (int j = 0; j < NM; j++) {
-      mk[a][j] = P->mk[a][j];
-      mcd[a][j] = P->mcd[a][j];
-      ma[a][j] = P->ma[a][j];
-      q[a][j] = 0.f;
-      v[a][j] = 0.f;
+      mk[a][j] = (T)P->mk[a][j];
+      mcd[a][j] = (T)P->mcd[a][j];
+      ma[a][j] = (T)P->ma[a][j];
+      q[a][j] = T(0);
+      v[a][j] = T(0);
     }
   // the kick e.vx = 0.01 m/s goes into the first x mode at the first run (cutting.js:164)
-  v[0][0] = 0.01f;
-  float x = 0.f, y = 0.f, vxs = 0.01f, vys = 0.f;
+  v[0][0] = T(0.01);
+  T x = T(0), y = T(0), vxs = T(0.01), vys = T(0);
 
-  const float hmax = P->hmax, mc = P->mc, dtf = P->dtf;
-  const bool size_effect = mc != 0.f;
+  const T hmax = (T)P->hmax, mc = (T)P->mc, dt = (T)P->dt;
+  const bool size_effect = P->mc != 0.0;
   const bool pd = pdK != 0.0;
   const int nsteps = P->nsteps, decim = P->decim, ts_c0 = P->ts_c0, h0 = P->hist_h0;
   int pr = 0, phc = 0, dcnt = 0, tcount = 0, hcount = 0, eng = 0;
@@ -170,8 +196,8 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   double sx = 0.0, sy = 0.0, sxx = 0.0, syy = 0.0, shx = 0.0, shy = 0.0;
 
   for (int step = 0; step < nsteps; step++) {
-    const float xm = x * 1e3f, ym = y * 1e3f;  // tool position [mm]
-    float Fx = 0.f, Fy = 0.f;
+    const T xm = x * T(1e3), ym = y * T(1e3);  // tool position [mm]
+    T Fx = T(0), Fy = T(0);
     int p = pr;  // position of tooth i: pr + i*spt (mod spr)
 #pragma unroll
     for (int i = 0; i < kMaxTeeth; i++) {
@@ -188,32 +214,30 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
         any |= act[s];
       }
       if (__any_sync(kFull, any)) {
-        const float2 sc = table[p];  // sin, cos of p*dphi (same address for all lanes)
+        const typename A::V2 sc = table[p];  // sin, cos of p*dphi (one address per warp)
 #pragma unroll
         for (int s = 0; s < SLOTS; s++) {
           if (act[s]) {
             // phi = p*dphi - lag: rotate the table entry by the slice's helix lag
-            const float sn = fmaf(sc.x, cL[s], -sc.y * sL[s]);
-            const float cs = fmaf(sc.y, cL[s], sc.x * sL[s]);
+            const T sn = A::madd(sc.x, cL[s], -sc.y * sL[s]);
+            const T cs = A::madd(sc.y, cL[s], sc.x * sL[s]);
             // feed u = [1, 0]: edge normal n = (sin phi, cos phi), tangent t = (cos, -sin)
-            const float rn = fmaf(xm, sn, fmaf(ym, cs, dRr[i]));
+            const T rn = A::madd(xm, sn, A::madd(ym, cs, dRr[i]));
             float* cell = ring + base[s] + jj[s];
-            const float prev = *cell;
-            const float feedH = fzk[s] * sn;
-            float h = (feedH + rn) - prev;
-            if (h <= 0.f) {
-              *cell = prev - feedH;  // out of cut: the old surface survives one more feed
+            const T prev = (T)*cell;
+            const T feedH = fzk[s] * sn;
+            T h = (feedH + rn) - prev;
+            if (h <= T(0)) {
+              *cell = (float)(prev - feedH);  // out of cut: the old surface survives
             } else {
-              *cell = rn;
-              h = fminf(h, hmax);
-              float kse = h;  // se * h
-              if (size_effect)
-                kse = h * exp2f(mc * (kLog2HRef - __log2f(fmaxf(h, kHMin))));
-              const float Ft = fmaf(ktb[s], kse, kteb[s]);
-              float Fr = fmaf(krb[s], kse, kreb[s]);
-              if (pd) Fr = fmaf(pdc[s], fmaf(vxs, sn, vys * cs), Fr);
-              Fx = fmaf(-Ft, cs, fmaf(-Fr, sn, Fx));
-              Fy = fmaf(Ft, sn, fmaf(-Fr, cs, Fy));
+              *cell = (float)rn;
+              if (h > hmax) h = hmax;  // (a NaN chip stays NaN, as in the reference)
+              const T kse = size_effect ? A::size_effect(h, mc) : h;  // se * h
+              const T Ft = A::madd(ktb[s], kse, kteb[s]);
+              T Fr = A::madd(krb[s], kse, kreb[s]);
+              if (pd) Fr = A::madd(pdc[s], A::madd(vxs, sn, vys * cs), Fr);
+              Fx = A::madd(-Ft, cs, A::madd(-Fr, sn, Fx));
+              Fy = A::madd(Ft, sn, A::madd(-Fr, cs, Fy));
               eng++;
             }
           }
@@ -225,15 +249,17 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     Fx = warp_sum(Fx);
     Fy = warp_sum(Fy);
     // modal integration, semi-implicit Euler; padded modes have k = c = dt/m = 0
-    float xs = 0.f, ys = 0.f, vxa = 0.f, vya = 0.f;
+    T xs = T(0), ys = T(0), vxa = T(0), vya = T(0);
 #pragma unroll
     for (int j = 0; j < NM; j++) {
-      v[0][j] = fmaf(fmaf(-mcd[0][j], v[0][j], fmaf(-mk[0][j], q[0][j], Fx)), ma[0][j], v[0][j]);
-      q[0][j] = fmaf(v[0][j], dtf, q[0][j]);
+      v[0][j] = A::madd(A::madd(-mcd[0][j], v[0][j], A::madd(-mk[0][j], q[0][j], Fx)), ma[0][j],
+                        v[0][j]);
+      q[0][j] = A::madd(v[0][j], dt, q[0][j]);
       xs += q[0][j];
       vxa += v[0][j];
-      v[1][j] = fmaf(fmaf(-mcd[1][j], v[1][j], fmaf(-mk[1][j], q[1][j], Fy)), ma[1][j], v[1][j]);
-      q[1][j] = fmaf(v[1][j], dtf, q[1][j]);
+      v[1][j] = A::madd(A::madd(-mcd[1][j], v[1][j], A::madd(-mk[1][j], q[1][j], Fy)), ma[1][j],
+                        v[1][j]);
+      q[1][j] = A::madd(v[1][j], dt, q[1][j]);
       ys += q[1][j];
       vya += v[1][j];
     }
@@ -242,18 +268,18 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     vxs = vxa;
     vys = vya;
     if (++pr == spr) pr = 0;
-    if (++phc == spt) {  // once-per-tooth sample (cutting.js:266-268)
+    if (++phc == spt) {  // once-per-tooth sample (cutting.js:266-268), Float32Array
       phc = 0;
       if (tcount - ts_c0 == lane) {
-        tsx = x;
-        tsy = y;
+        tsx = (float)x;
+        tsy = (float)y;
       }
       tcount++;
     }
     if (++dcnt == decim) {  // decimated history (cutting.js:288-292), FP64 window sums
       dcnt = 0;
       if (hcount >= h0) {
-        const double hx = (double)(x * 1e6f), hy = (double)(y * 1e6f);
+        const double hx = (double)(float)((double)x * 1e6), hy = (double)(float)((double)y * 1e6);
         if (hcount == h0) {
           shx = hx;
           shy = hy;
@@ -284,13 +310,16 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     const double vv = warp_sum(ex * ex + ey * ey);
     const double once = sqrt(vv / n) * 1e6;
     const double md = P->hist_m ? (double)P->hist_m : 1.0;
-    const double w = fmax(0.0, (sxx - sx * sx / md) + (syy - sy * sy / md));
+    double w = (sxx - sx * sx / md) + (syy - sy * sy / md);
+    if (w < 0.0) w = 0.0;  // rounding of the one-pass form; a NaN (run-away cut) stays NaN
     const double amp = sqrt(w / md);
     res.once = once;
     res.amp = amp;
     res.index = once / (amp + 0.05);
   }
-  res.status = (isfinite(x) && isfinite(y) && isfinite(res.index)) ? MCS_OK : MCS_ERR_DIVERGED;
+  res.status = (isfinite((double)x) && isfinite((double)y) && isfinite(res.index))
+                   ? MCS_OK
+                   : MCS_ERR_DIVERGED;
   return res;
 }
 
@@ -301,7 +330,7 @@ __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane
 }
 
 // Persistent solve: each warp takes points from the queue and runs timeDomainLimit.
-template <int SLOTS, int NM>
+template <typename T, int SLOTS, int NM>
 __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restrict__ pts,
                                                       const int32_t* __restrict__ order, int n,
                                                       DevOpts o, mcs_result* __restrict__ out,
@@ -317,8 +346,8 @@ __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restr
     if (w >= (unsigned)n) break;
     const int pi = order[w];
     const PointParams* P = pts + pi;
-    float2* table = reinterpret_cast<float2*>(smem);
-    float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr));
+    auto* table = reinterpret_cast<typename Arith<T>::V2*>(smem);
+    float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr, sizeof(T) == 8));
     mcs_result r;
     r.status = MCS_OK;
     r.trials = 0;
@@ -330,9 +359,9 @@ __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restr
     if (read_cancel(cancel, lane)) {
       r.status = MCS_ERR_CANCELLED;
     } else {
-      build_table(P, table, lane);
+      build_table<T>(P, table, lane);
       auto chatter = [&](double ap, bool& ok) -> bool {
-        const TrialOut t = simulate_trial<SLOTS, NM>(P, ap, table, ring, lane);
+        const TrialOut t = simulate_trial<T, SLOTS, NM>(P, ap, table, ring, lane);
         r.trials++;
         r.evals += t.evals;
         r.engaged += t.engaged;
@@ -373,7 +402,7 @@ __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restr
 }
 
 // Batch of independent chatterAt trials (decision replay at given depths).
-template <int SLOTS, int NM>
+template <typename T, int SLOTS, int NM>
 __global__ void __launch_bounds__(kWarp) trials_kernel(const PointParams* __restrict__ pts,
                                                        const TrialItem* __restrict__ items,
                                                        int n, double chatter_idx,
@@ -388,10 +417,10 @@ __global__ void __launch_bounds__(kWarp) trials_kernel(const PointParams* __rest
     if (w >= (unsigned)n) break;
     const TrialItem it = items[w];
     const PointParams* P = pts + it.point;
-    float2* table = reinterpret_cast<float2*>(smem);
-    float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr));
-    build_table(P, table, lane);
-    const TrialOut t = simulate_trial<SLOTS, NM>(P, it.ap, table, ring, lane);
+    auto* table = reinterpret_cast<typename Arith<T>::V2*>(smem);
+    float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr, sizeof(T) == 8));
+    build_table<T>(P, table, lane);
+    const TrialOut t = simulate_trial<T, SLOTS, NM>(P, it.ap, table, ring, lane);
     if (lane == 0) {
       mcs_trial_result r;
       r.index = t.index;
@@ -405,19 +434,20 @@ __global__ void __launch_bounds__(kWarp) trials_kernel(const PointParams* __rest
   }
 }
 
-template <int SLOTS, int NM>
+template <typename T, int SLOTS, int NM>
 void* solve_fn() {
-  return reinterpret_cast<void*>(&solve_kernel<SLOTS, NM>);
+  return reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM>);
 }
-template <int SLOTS, int NM>
+template <typename T, int SLOTS, int NM>
 void* trials_fn() {
-  return reinterpret_cast<void*>(&trials_kernel<SLOTS, NM>);
+  return reinterpret_cast<void*>(&trials_kernel<T, SLOTS, NM>);
 }
 
 void* pick(bool solve, const KernelShape& s) {
-#define MCS_PICK(SL, NMV)                                      \
-  if (s.slots == SL && s.modes == NMV)                         \
-    return solve ? solve_fn<SL, NMV>() : trials_fn<SL, NMV>();
+#define MCS_PICK(SL, NMV)                                                              \
+  if (s.slots == SL && s.modes == NMV)                                                 \
+    return s.fp64 ? (solve ? solve_fn<double, SL, NMV>() : trials_fn<double, SL, NMV>()) \
+                  : (solve ? solve_fn<float, SL, NMV>() : trials_fn<float, SL, NMV>());
   MCS_PICK(1, 1)
   MCS_PICK(1, 2)
   MCS_PICK(1, 3)
@@ -433,10 +463,11 @@ void* pick(bool solve, const KernelShape& s) {
 }  // namespace
 
 int set_smem_limits() {
+  for (int fp = 0; fp < 2; fp++)
   for (int sl = 1; sl <= kMaxSlots; sl++)
     for (int nm = 1; nm <= kMaxModes; nm++)
       for (int k = 0; k < 2; k++) {
-        void* f = pick(k == 0, KernelShape{sl, nm});
+        void* f = pick(k == 0, KernelShape{sl, nm, fp});
         cudaError_t e =
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerWarp);
         if (e != cudaSuccess) return (int)e;

@@ -82,7 +82,7 @@ class Opts(C.Structure):
     _fields_ = [("a_min", C.c_double), ("a_max", C.c_double), ("iters", C.c_int32),
                 ("revs", C.c_int32), ("nonlinear", C.c_int32), ("honor_runout", C.c_int32),
                 ("steps_per_tooth", C.c_int32), ("slices", C.c_int32),
-                ("chatter_idx", C.c_double)]
+                ("chatter_idx", C.c_double), ("precision", C.c_int32), ("pad", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -176,7 +176,8 @@ def make_setup(tool, mat, arc: Sequence[float], fz: float) -> Setup:
 
 def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
     """timeDomainLimit/chatterAt options (src/stabtd.js:14,24) with the reference defaults,
-    plus the explicit extensions honorRunout, stepsPerTooth, slices and chatterIdx."""
+    plus the explicit extensions honorRunout, stepsPerTooth, slices, chatterIdx and
+    precision ("fp32": FP32 force law and modal integration, "fp64": FP64)."""
     d = dict(DEFAULTS)
     if o:
         d.update(o)
@@ -185,7 +186,19 @@ def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
                 1 if d.get("nonlinear", True) is not False else 0,
                 1 if d.get("honorRunout", False) else 0,
                 int(d.get("stepsPerTooth", 0) or 0), int(d.get("slices", 0) or 0),
-                float(d.get("chatterIdx", CHATTER_IDX)))
+                float(d.get("chatterIdx", CHATTER_IDX)), precision_code(d.get("precision")), 0)
+
+
+FP32 = 0
+FP64 = 1
+
+
+def precision_code(p) -> int:
+    if p is None or p in ("fp32", "f32", 0):
+        return FP32
+    if p in ("fp64", "f64", 1):
+        return FP64
+    raise ValueError(f"precision must be 'fp32' or 'fp64', not {p!r}")
 
 
 def array_of(ctype, items: Sequence) -> C.Array:
@@ -239,7 +252,8 @@ POINT_DTYPE = np.dtype([("setup", "<u4"), ("modal", "<u4"), ("S", "<f8")])
 TRIAL_DTYPE = np.dtype([("point", "<u4"), ("pad", "<u4"), ("ap", "<f8")])
 OPTS_DTYPE = np.dtype([("a_min", "<f8"), ("a_max", "<f8"), ("iters", "<i4"), ("revs", "<i4"),
                        ("nonlinear", "<i4"), ("honor_runout", "<i4"),
-                       ("steps_per_tooth", "<i4"), ("slices", "<i4"), ("chatter_idx", "<f8")])
+                       ("steps_per_tooth", "<i4"), ("slices", "<i4"), ("chatter_idx", "<f8"),
+                       ("precision", "<i4"), ("pad", "<i4")])
 for _d, _c in ((MODAL_DTYPE, Modal), (SETUP_DTYPE, Setup), (POINT_DTYPE, Point),
                (TRIAL_DTYPE, Trial), (OPTS_DTYPE, Opts)):
     assert _d.itemsize == C.sizeof(_c), (_d, _c)

@@ -35,7 +35,7 @@ def chatterAt(tool, modal, mat, S, arc, fz, ap, opts: Mapping[str, Any] | None =
     setups, modals, points = _one(tool, modal, mat, S, arc, fz)
     trials = np.array([(0, 0, float(ap))], dtype=A.TRIAL_DTYPE)
     r = _ctx(ctx).chatter_at(setups, modals, points, trials, A.make_opts(opts))
-    if r["status"][0] not in (A.MCS_OK,):
+    if r["status"][0] not in (A.MCS_OK, A.MCS_ERR_DIVERGED):
         raise MCSError(int(r["status"][0]), "trial did not complete")
     return bool(r["chatter"][0])
 
@@ -53,7 +53,9 @@ def timeDomainLimit(tool, modal, mat, S, arc, fz, opts: Mapping[str, Any] | None
     """Critical depth by bisection: {alim, bracket: [stable, chatter]} (stabtd.js:24-32)."""
     setups, modals, points = _one(tool, modal, mat, S, arc, fz)
     r = _ctx(ctx).solve(setups, modals, points, A.make_opts(opts))[0]
-    if r["status"] != A.MCS_OK:
+    # a run-away trial (MCS_ERR_DIVERGED) decides "stable" as the reference's NaN > 0.45
+    # does; the result is returned like the reference's
+    if r["status"] not in (A.MCS_OK, A.MCS_ERR_DIVERGED):
         raise MCSError(int(r["status"]), "point did not complete")
     return A.result_dict(r)
 

@@ -58,11 +58,50 @@ def run(wl: W.Workload, idx, threads: int, out: Path):
     setups, modals, P, pts = as_ctypes(wl, idx)
     t = time.time()
     res, tr = O.solve_batch(setups, modals, P, wl.opts, nthreads=threads, traces=True)
+    sens = [sensitivity(wl, pts, res, tr, threads, eps) for eps in SENS_LEVELS]
     dt = time.time() - t
     np.savez_compressed(out, setups=wl.setups, modals=wl.modals, points=pts,
                         index=idx_orig, opts=A.opts_record(wl.opts), results=res,
-                        traces=tr)
-    print(f"{out.name}: {len(idx)} points in {dt:.1f} s", flush=True)
+                        traces=tr, sens_levels=np.array(SENS_LEVELS),
+                        sens_index=np.stack([s[0] for s in sens]),
+                        sens_flip=np.stack([s[1] for s in sens]))
+    flips = ", ".join(f"{int(s[1].sum())} at {e:g}" for e, s in zip(SENS_LEVELS, sens))
+    print(f"{out.name}: {len(idx)} points in {dt:.1f} s; of {int((tr['ap'] > 0).sum())} "
+          f"traced trials these flip under a feed perturbation: {flips}", flush=True)
+
+
+# relative feed perturbations probed: one FP32 rounding (1e-7) up to what an FP32
+# trajectory of ~1e5 steps accumulates (1e-5)
+SENS_LEVELS = [1e-7, 1e-6, 3e-6, 1e-5]
+
+
+def sensitivity(wl, pts, res, tr, threads, eps):
+    """How the FP64 reference's own decision at each traced depth reacts to feeds scaled by
+    (1 +- eps): the largest index change and whether the decision flips.  A trial whose
+    decision flips under a rounding-sized input change (1e-7: one FP32 rounding; 1e-6: the
+    error an FP32 trajectory accumulates) is ill-conditioned: no integration in another
+    precision or operation order can be expected to reproduce it."""
+    per = tr.shape[1]
+    rows = [(p, j) for p in range(len(res)) for j in range(int(res["trials"][p]))]
+    trials = np.zeros(len(rows), dtype=A.TRIAL_DTYPE)
+    for i, (p, j) in enumerate(rows):
+        trials[i] = (p, 0, tr[p, j]["ap"])
+    T = (A.Trial * len(rows)).from_buffer_copy(trials.tobytes())
+    P = (A.Point * len(pts)).from_buffer_copy(pts.tobytes())
+    modals = [A.Modal.from_buffer_copy(r.tobytes()) for r in wl.modals]
+    dmax = np.zeros((len(res), per))
+    flip = np.zeros((len(res), per), dtype=bool)
+    for sgn in (+1, -1):
+        st = wl.setups.copy()
+        st["fz"] *= 1 + sgn * eps
+        setups = [A.Setup.from_buffer_copy(r.tobytes()) for r in st]
+        out = O.chatter_batch(setups, modals, P, T, wl.opts, nthreads=threads)
+        for i, (p, j) in enumerate(rows):
+            a, b = tr[p, j]["index"], out["index"][i]
+            d = abs(b - a) if np.isfinite(a) and np.isfinite(b) else np.inf
+            dmax[p, j] = max(dmax[p, j], d)
+            flip[p, j] |= bool(out["chatter"][i]) != bool(tr[p, j]["chatter"])
+    return dmax, flip
 
 
 def edge_workload() -> W.Workload:
