@@ -233,6 +233,28 @@ int mcs_job_wait(mcs_job* job); /* MCS_OK, or MCS_ERR_CANCELLED when cancelled *
 void mcs_job_free(mcs_job* job);
 
 /*
+ * Solve without allocating: the same batched timeDomainLimit as mcs_solve, for callers
+ * that must not allocate GPU memory -- code that runs while a CUDA graph is being built
+ * on another stream, real-time loops where the device-wide synchronisation of
+ * cudaMalloc/cudaFree would stall other work, or hosts whose device memory is owned by
+ * another allocator.  This entry point has no counterpart in the reference.
+ *
+ * Inputs and outputs are the caller's host arrays, as for mcs_solve.  The per-point
+ * parameters, the work queue and the device copy of the results live in a preallocated
+ * scratch area that every GPU loading the library holds until the process exits
+ * (about 0.5 MB), so a call solves at most MCS_NOALLOC_MAX_POINTS points; larger batches
+ * fail with MCS_ERR_ARG.  The first call on a device looks the scratch area up (make it
+ * before any stream capture).  All calls share the area: the library serialises them
+ * per device and each call waits for its work, so its calls never overlap on the GPU;
+ * work that touched the area concurrently would race.  It calls no cudaMalloc, cudaFree
+ * or other allocating routine.
+ */
+#define MCS_NOALLOC_MAX_POINTS 1024
+int mcs_solve_noalloc(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,
+                      const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                      size_t n_points, const mcs_opts* opts, mcs_result* out);
+
+/*
  * Zero-order lobes (sld.js:23-61) read at spindle speeds (alimAt, sld.js:64-76):
  * alim[q * n_rpm + r] for query q at rpm[r]; +inf where no lobe covers the speed.
  */

@@ -928,3 +928,120 @@ int mcs_lobes_alim(mcs_ctx* c, const mcs_modal* modals, size_t n_modals,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free solve
+// mcs_solve without device allocations: the per-point parameters, the work order, the
+// queue counter and the device copy of the results sit in this file-scope array, which
+// every device that loads the library keeps until exit.  Host code must not use the
+// array's name as an address: its device address is looked up once per device with
+// cudaGetSymbolAddress and passed to the kernels.
+namespace {
+
+constexpr size_t kNaMax = MCS_NOALLOC_MAX_POINTS;
+constexpr size_t kNaAlign = 256;
+constexpr size_t na_up(size_t b) { return (b + kNaAlign - 1) & ~(kNaAlign - 1); }
+constexpr size_t kNaQueueOff = 0;
+constexpr size_t kNaOrderOff = kNaAlign;
+constexpr size_t kNaParamsOff = kNaOrderOff + na_up(sizeof(int32_t) * kNaMax);
+constexpr size_t kNaResultsOff = kNaParamsOff + na_up(sizeof(PointParams) * kNaMax);
+constexpr size_t kNaBytes = kNaResultsOff + na_up(sizeof(mcs_result) * kNaMax);
+constexpr int kNaMaxDevices = 64;
+constexpr int kNaChunk = 32;  // points prepared per host-to-device copy (on the stack)
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+std::mutex g_na_setup_mu;
+unsigned char* g_na_ptr[kNaMaxDevices] = {};
+std::mutex g_na_dev_mu[kNaMaxDevices];
+
+// Device address of the scratch array on the current device (looked up on first use).
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kNaMaxDevices)
+    return fail(MCS_ERR_UNSUPPORTED, "device %d: the allocation-free path serves devices "
+                "0..%d", device, kNaMaxDevices - 1);
+  std::lock_guard<std::mutex> lk(g_na_setup_mu);
+  if (!g_na_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(MCS_ERR_CUDA, "cudaGetSymbolAddress of the scratch area failed: %s",
+                  cudaGetErrorString(e));
+    g_na_ptr[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_na_ptr[device];
+  return MCS_OK;
+}
+
+}  // namespace
+
+extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
+                                 const mcs_modal* modals, size_t n_modals,
+                                 const mcs_point* points, size_t n_points, const mcs_opts* o,
+                                 mcs_result* out) {
+  if (!c) return fail(MCS_ERR_ARG, "ctx is NULL");
+  if (n_points && !out) return fail(MCS_ERR_ARG, "out is NULL");
+  if (n_points > kNaMax)
+    return fail(MCS_ERR_ARG, "%zu points exceed the %zu the preallocated scratch area holds "
+                "(MCS_NOALLOC_MAX_POINTS); split the batch or use mcs_solve",
+                n_points, kNaMax);
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
+  if (rc) return rc;
+  if (n_points == 0) return MCS_OK;
+  unsigned char* base = nullptr;
+  if ((rc = noalloc_scratch(c->device, &base))) return rc;
+  std::lock_guard<std::mutex> dev_lk(g_na_dev_mu[c->device]);
+  cudaStream_t st = c->stream;
+  auto* d_queue = reinterpret_cast<unsigned int*>(base + kNaQueueOff);
+  auto* d_order = reinterpret_cast<int32_t*>(base + kNaOrderOff);
+  auto* d_params = reinterpret_cast<PointParams*>(base + kNaParamsOff);
+  auto* d_results = reinterpret_cast<mcs_result*>(base + kNaResultsOff);
+
+  // prepare on the host in stack-sized chunks and copy each into the scratch area
+  PointParams chunk[kNaChunk];
+  double cost[kNaMax];
+  int32_t order[kNaMax];
+  int smem = 0, slots = 1, modes = 1;
+  for (size_t i0 = 0; i0 < n_points; i0 += kNaChunk) {
+    const size_t m = std::min<size_t>(kNaChunk, n_points - i0);
+    for (size_t j = 0; j < m; j++) {
+      const size_t i = i0 + j;
+      Prepared pr;
+      rc = prepare_point(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,
+                         o->a_max, pr);
+      if (rc) return fail(rc, "point %zu: %s", i, g_last_error.c_str());
+      chunk[j] = pr.pp;
+      cost[i] = pr.cost;
+      smem = std::max(smem, pr.pp.smem_bytes);
+      slots = std::max(slots, slots_for(pr.pp.nz_max));
+      modes = std::max(modes, pr.modes);
+    }
+    MCS_CUDA(cudaMemcpyAsync(d_params + i0, chunk, sizeof(PointParams) * m,
+                             cudaMemcpyHostToDevice, st));
+    MCS_CUDA(cudaStreamSynchronize(st));  // the chunk buffer is reused
+  }
+  // largest first, for the persistent warps' load balance
+  for (size_t i = 0; i < n_points; i++) order[i] = (int32_t)i;
+  std::sort(order, order + n_points, [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+  MCS_CUDA(cudaMemcpyAsync(d_order, order, sizeof(int32_t) * n_points, cudaMemcpyHostToDevice,
+                           st));
+  // the queue counter must start at zero; the area keeps the previous call's contents
+  MCS_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
+  const KernelShape shape{slots, modes, o->precision == MCS_FP64 ? 1 : 0};
+  smem = (smem + 15) & ~15;
+  int bps = 0;
+  const int orc = occupancy_solve(shape, smem, &bps);
+  if (orc != 0)
+    return fail(MCS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString((cudaError_t)orc));
+  if (bps < 1) return fail(MCS_ERR_UNSUPPORTED, "a %d-byte warp does not fit on an SM", smem);
+  const int grid = (int)std::min<long long>((long long)n_points, (long long)bps * c->sms);
+  const int lrc = launch_solve(shape, grid, smem, st, d_params, d_order, (int)n_points,
+                               dev_opts(o), d_results, d_queue, nullptr, nullptr);
+  if (lrc != 0)
+    return fail(MCS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString((cudaError_t)lrc));
+  MCS_CUDA(cudaMemcpyAsync(out, d_results, sizeof(mcs_result) * n_points,
+                           cudaMemcpyDeviceToHost, st));
+  MCS_CUDA(cudaStreamSynchronize(st));
+  return MCS_OK;
+}

@@ -22,7 +22,7 @@ EXPORTS = (
     "mcs_default_opts", "mcs_last_error", "mcs_create", "mcs_destroy", "mcs_stream",
     "mcs_solve", "mcs_chatter_at", "mcs_plan_create", "mcs_plan_execute", "mcs_plan_results",
     "mcs_plan_info_get", "mcs_plan_destroy", "mcs_solve_async", "mcs_job_poll",
-    "mcs_job_cancel", "mcs_job_wait", "mcs_job_free", "mcs_lobes_alim",
+    "mcs_job_cancel", "mcs_job_wait", "mcs_job_free", "mcs_lobes_alim", "mcs_solve_noalloc",
 )
 
 _LIB = None
@@ -72,6 +72,7 @@ def load(path: Path | str | None = None):
         L.mcs_job_free.argtypes = [vp]
         L.mcs_job_free.restype = None
         L.mcs_lobes_alim.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, vp]
+        L.mcs_solve_noalloc.argtypes = batch + [vp]
         for name in EXPORTS:
             if name not in ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free"):
                 getattr(L, name).restype = C.c_int
