@@ -125,6 +125,7 @@ struct Prepared {
   PointParams pp;
   double cost;
   int modes;  // max modes per axis
+  int nl;     // size effect or process damping present
 };
 
 int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const mcs_opts& o,
@@ -182,6 +183,7 @@ int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const m
     }
   }
   out.modes = std::max(nx, ny);
+  out.nl = (P.mc != 0.0 || P.Ci != 0.0) ? 1 : 0;
   P.N = N;
   P.spt = spt;
   P.spr = N * spt;
@@ -318,8 +320,9 @@ namespace {
 // Orders the work items by cost (largest first) and groups them into buckets of similar
 // shared-memory need, each launched as its own persistent grid.
 int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
-                 const std::vector<int>& slots, const std::vector<int>& modes, bool trials,
-                 int fp64, std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
+                 const std::vector<int>& slots, const std::vector<int>& modes,
+                 const std::vector<int>& nls, bool trials, int fp64,
+                 std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
   const size_t n = smem.size();
   std::vector<int32_t> idx(n);
   std::iota(idx.begin(), idx.end(), 0);
@@ -335,16 +338,18 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     Bucket b;
     const int top = smem[idx[i]];
     size_t j = i;
-    int sl = 1, nm = 1;
+    int sl = 1, nm = 1, nl = 0;
     while (j < n && (double)smem[idx[j]] * ratio >= top) {
       sl = std::max(sl, slots[idx[j]]);
       nm = std::max(nm, modes[idx[j]]);
+      nl = std::max(nl, nls[idx[j]]);
       j++;
     }
     if ((int)buckets.size() == kMaxBuckets - 1) {  // last bucket takes the rest
       for (size_t k = j; k < n; k++) {
         sl = std::max(sl, slots[idx[k]]);
         nm = std::max(nm, modes[idx[k]]);
+        nl = std::max(nl, nls[idx[k]]);
       }
       j = n;
     }
@@ -353,7 +358,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     b.offset = (int)order.size();
     b.count = (int)seg.size();
     b.smem = (top + 15) & ~15;
-    b.shape = KernelShape{sl, nm, fp64};
+    b.shape = KernelShape{sl, nm, fp64, nl};
     order.insert(order.end(), seg.begin(), seg.end());
     int bps = 0;
     const int rc = trials ? occupancy_trials(b.shape, b.smem, &bps)
@@ -463,7 +468,7 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
   if (rc) return rc;
   std::vector<PointParams> pp(n_points);
-  std::vector<int> smem(n_points), slots(n_points), modes(n_points);
+  std::vector<int> smem(n_points), slots(n_points), modes(n_points), nls(n_points);
   std::vector<double> cost(n_points);
   for (size_t i = 0; i < n_points; i++) {
     Prepared pr;
@@ -474,13 +479,14 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
     smem[i] = pr.pp.smem_bytes;
     slots[i] = slots_for(pr.pp.nz_max);
     modes[i] = pr.modes;
+    nls[i] = pr.nl;
     cost[i] = pr.cost;
   }
   mcs_plan* pl = new mcs_plan();
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
-  rc = make_buckets(ctx, smem, cost, slots, modes, false, o->precision == MCS_FP64, order,
+  rc = make_buckets(ctx, smem, cost, slots, modes, nls, false, o->precision == MCS_FP64, order,
                     pl->buckets);
   if (rc) {
     plan_free(pl);
@@ -715,7 +721,7 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
   for (size_t i = 0; i < n_trials; i++)
     deepest[trials[i].point] = std::max(deepest[trials[i].point], trials[i].ap);
   std::vector<PointParams> pp(n_points);
-  std::vector<int> modes(n_points);
+  std::vector<int> modes(n_points), pnl(n_points);
   for (size_t i = 0; i < n_points; i++) {
     Prepared pr;
     ap_max = deepest[i] > 0 ? deepest[i] : o->a_min;
@@ -724,8 +730,9 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
     if (rc) return fail(rc, "point %zu: %s", i, g_last_error.c_str());
     pp[i] = pr.pp;
     modes[i] = pr.modes;
+    pnl[i] = pr.nl;
   }
-  std::vector<int> smem(n_trials), slots(n_trials), tmodes(n_trials);
+  std::vector<int> smem(n_trials), slots(n_trials), tmodes(n_trials), tnl(n_trials);
   std::vector<double> cost(n_trials);
   std::vector<TrialItem> items_by_idx(n_trials);
   for (size_t i = 0; i < n_trials; i++) {
@@ -734,6 +741,7 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
     smem[i] = table_bytes(P.spr, o->precision == MCS_FP64) + 4 * nz * P.lpad;
     slots[i] = slots_for(nz);
     tmodes[i] = modes[trials[i].point];
+    tnl[i] = pnl[trials[i].point];
     cost[i] = (double)P.nsteps * (24.0 + 40.0 * P.N * slots[i]);
     items_by_idx[i] = TrialItem{(int32_t)trials[i].point, (int32_t)i, trials[i].ap};
   }
@@ -742,7 +750,7 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
   pl->trials = true;
   pl->n = n_trials;
   std::vector<int32_t> order;
-  rc = make_buckets(c, smem, cost, slots, tmodes, true, o->precision == MCS_FP64, order,
+  rc = make_buckets(c, smem, cost, slots, tmodes, tnl, true, o->precision == MCS_FP64, order,
                     pl->buckets);
   std::vector<TrialItem> items(n_trials);
   for (size_t k = 0; k < order.size(); k++) items[k] = items_by_idx[order[k]];
@@ -1002,7 +1010,7 @@ extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_s
   PointParams chunk[kNaChunk];
   double cost[kNaMax];
   int32_t order[kNaMax];
-  int smem = 0, slots = 1, modes = 1;
+  int smem = 0, slots = 1, modes = 1, nl = 0;
   for (size_t i0 = 0; i0 < n_points; i0 += kNaChunk) {
     const size_t m = std::min<size_t>(kNaChunk, n_points - i0);
     for (size_t j = 0; j < m; j++) {
@@ -1016,6 +1024,7 @@ extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_s
       smem = std::max(smem, pr.pp.smem_bytes);
       slots = std::max(slots, slots_for(pr.pp.nz_max));
       modes = std::max(modes, pr.modes);
+      nl = std::max(nl, pr.nl);
     }
     MCS_CUDA(cudaMemcpyAsync(d_params + i0, chunk, sizeof(PointParams) * m,
                              cudaMemcpyHostToDevice, st));
@@ -1028,7 +1037,7 @@ extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_s
                            st));
   // the queue counter must start at zero; the area keeps the previous call's contents
   MCS_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
-  const KernelShape shape{slots, modes, o->precision == MCS_FP64 ? 1 : 0};
+  const KernelShape shape{slots, modes, o->precision == MCS_FP64 ? 1 : 0, nl};
   smem = (smem + 15) & ~15;
   int bps = 0;
   const int orc = occupancy_solve(shape, smem, &bps);

@@ -73,6 +73,7 @@ struct KernelShape {
   int slots;  // 1 or 2
   int modes;  // 1..4
   int fp64;   // 0: FP32 force law and modal integration, 1: FP64
+  int nl;     // 1: size effect and/or process damping present
 };
 
 // Host launchers (mcs_kernels.cu).

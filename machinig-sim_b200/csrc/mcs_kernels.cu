@@ -97,7 +97,9 @@ __device__ __forceinline__ void build_table(const PointParams* __restrict__ P,
 }
 
 // One chatterAt trial at depth ap: configure + setEngagement + kick + run + chatterIndex.
-template <typename T, int SLOTS, int NM>
+// NL: size effect and process damping present (cutting.js:153-156,197,203); linear cuts
+// are compiled without them.
+template <typename T, int SLOTS, int NM, bool NL>
 __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
                                    const typename Arith<T>::V2* __restrict__ table,
                                    float* __restrict__ ring, int lane) {
@@ -118,11 +120,16 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     nz = ap > 0 ? min(maxs, (int)ceil(ap / dz)) : 0;
   }
   // process damping per slice, Ci*b/V_c (cutting.js:155-156,203)
-  const double pdK = P->Ci != 0.0 ? P->Ci * dz * 1e-3 / (P->omega * 1e-3) : 0.0;
+  const double pdK = NL && P->Ci != 0.0 ? P->Ci * dz * 1e-3 / (P->omega * 1e-3) : 0.0;
 
+  // Per slot: slice geometry, and the slot's phase in the revolution.  Tooth i of a slice
+  // whose engaged window starts at position p0 is in cut when j_i = (pr + i*spt - p0) mod
+  // spr < len.  With q = (pr - p0) mod spr = c*spt + r, j_i = ((c + i) mod N)*spt + r: the
+  // teeth in cut at a step are those with u = (c + i) mod N < U, U = ceil((len - r)/spt),
+  // so a lane visits only its own in-cut teeth, in rounds u = 0, 1, ...
   T sL[SLOTS], cL[SLOTS], ktb[SLOTS], kteb[SLOTS], krb[SLOTS], kreb[SLOTS], pdc[SLOTS],
       fzk[SLOTS];
-  int p0[SLOTS], len[SLOTS], base[SLOTS];
+  int p0[SLOTS], len[SLOTS], base[SLOTS], cph[SLOTS], rph[SLOTS];
 #pragma unroll
   for (int s = 0; s < SLOTS; s++) {
     const int k = lane + kWarp * s;
@@ -161,17 +168,19 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
       kteb[s] = (T)(P->Kte * b);
       krb[s] = (T)(P->Krc * b);
       kreb[s] = (T)(P->Kre * b);
-      pdc[s] = (T)(pdK * (b / dz) / r);
+      if (NL) pdc[s] = (T)(pdK * (b / dz) / r);
       fzk[s] = (T)(P->fz * kap);
     }
+    const int q = (spr - p0[s]) % spr;  // phase at pr = 0
+    cph[s] = q / spt;
+    rph[s] = q - cph[s] * spt;
   }
   // a fresh engine's surface is all zeros (cutting.js:68)
   for (int i = lane; i < nz * lpad; i += kWarp) ring[i] = 0.f;
   __syncwarp();
 
-  T dRr[kMaxTeeth];
-#pragma unroll
-  for (int i = 0; i < kMaxTeeth; i++) dRr[i] = (T)P->dR[i];
+  // lane i < N holds tooth i's runout offset (read by shuffle)
+  const T dRl = lane < kMaxTeeth ? (T)P->dR[lane] : T(0);
   T mk[2][NM], mcd[2][NM], ma[2][NM], q[2][NM], v[2][NM];
 #pragma unroll
   for (int a = 0; a < 2; a++)
@@ -188,63 +197,54 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   T x = T(0), y = T(0), vxs = T(0.01), vys = T(0);
 
   const T hmax = (T)P->hmax, mc = (T)P->mc, dt = (T)P->dt;
-  const bool size_effect = P->mc != 0.0;
-  const bool pd = pdK != 0.0;
+  const bool size_effect = NL && P->mc != 0.0;
+  const bool pd = NL && pdK != 0.0;
   const int nsteps = P->nsteps, decim = P->decim, ts_c0 = P->ts_c0, h0 = P->hist_h0;
-  int pr = 0, phc = 0, dcnt = 0, tcount = 0, hcount = 0, eng = 0;
-  float tsx = 0.f, tsy = 0.f;
-  double sx = 0.0, sy = 0.0, sxx = 0.0, syy = 0.0, shx = 0.0, shy = 0.0;
+  int phc = 0, dcnt = 0, tcount = 0, hcount = 0, eng = 0;
+  float tsx = 0.f, tsy = 0.f, shx = 0.f, shy = 0.f;
+  // FP64 sums of the history window, one per lane: sum dx, sum dy, sum dx^2, sum dy^2
+  double acc = 0.0;
 
   for (int step = 0; step < nsteps; step++) {
     const T xm = x * T(1e3), ym = y * T(1e3);  // tool position [mm]
     T Fx = T(0), Fy = T(0);
-    int p = pr;  // position of tooth i: pr + i*spt (mod spr)
 #pragma unroll
-    for (int i = 0; i < kMaxTeeth; i++) {
-      if (i >= N) break;
-      int jj[SLOTS];
-      bool act[SLOTS];
-      bool any = false;
-#pragma unroll
-      for (int s = 0; s < SLOTS; s++) {
-        int j = p - p0[s];
-        if (j < 0) j += spr;
-        jj[s] = j;
-        act[s] = j < len[s];
-        any |= act[s];
-      }
-      if (__any_sync(kFull, any)) {
-        const typename A::V2 sc = table[p];  // sin, cos of p*dphi (one address per warp)
-#pragma unroll
-        for (int s = 0; s < SLOTS; s++) {
-          if (act[s]) {
-            // phi = p*dphi - lag: rotate the table entry by the slice's helix lag
-            const T sn = A::madd(sc.x, cL[s], -sc.y * sL[s]);
-            const T cs = A::madd(sc.y, cL[s], sc.x * sL[s]);
-            // feed u = [1, 0]: edge normal n = (sin phi, cos phi), tangent t = (cos, -sin)
-            const T rn = A::madd(xm, sn, A::madd(ym, cs, dRr[i]));
-            float* cell = ring + base[s] + jj[s];
-            const T prev = (T)*cell;
-            const T feedH = fzk[s] * sn;
-            T h = (feedH + rn) - prev;
-            if (h <= T(0)) {
-              *cell = (float)(prev - feedH);  // out of cut: the old surface survives
-            } else {
-              *cell = (float)rn;
-              if (h > hmax) h = hmax;  // (a NaN chip stays NaN, as in the reference)
-              const T kse = size_effect ? A::size_effect(h, mc) : h;  // se * h
-              const T Ft = A::madd(ktb[s], kse, kteb[s]);
-              T Fr = A::madd(krb[s], kse, kreb[s]);
-              if (pd) Fr = A::madd(pdc[s], A::madd(vxs, sn, vys * cs), Fr);
-              Fx = A::madd(-Ft, cs, A::madd(-Fr, sn, Fx));
-              Fy = A::madd(Ft, sn, A::madd(-Fr, cs, Fy));
-              eng++;
-            }
+    for (int s = 0; s < SLOTS; s++) {
+      for (int u = 0; u < N; u++) {
+        const int j = u * spt + rph[s];
+        const bool act = j < len[s];
+        if (!__any_sync(kFull, act)) break;  // rounds are monotone: later ones are empty too
+        int i = u - cph[s];
+        if (i < 0) i += N;
+        const T dRi = __shfl_sync(kFull, dRl, i);
+        if (act) {
+          int p = p0[s] + j;  // table position of tooth i at this step
+          if (p >= spr) p -= spr;
+          const typename A::V2 sc = table[p];
+          // phi = p*dphi - lag: rotate the table entry by the slice's helix lag
+          const T sn = A::madd(sc.x, cL[s], -sc.y * sL[s]);
+          const T cs = A::madd(sc.y, cL[s], sc.x * sL[s]);
+          // feed u = [1, 0]: edge normal n = (sin phi, cos phi), tangent t = (cos, -sin)
+          const T rn = A::madd(xm, sn, A::madd(ym, cs, dRi));
+          float* cell = ring + base[s] + j;
+          const T prev = (T)*cell;
+          const T feedH = fzk[s] * sn;
+          T h = (feedH + rn) - prev;
+          if (h <= T(0)) {
+            *cell = (float)(prev - feedH);  // out of cut: the old surface survives
+          } else {
+            *cell = (float)rn;
+            if (h > hmax) h = hmax;  // (a NaN chip stays NaN, as in the reference)
+            const T kse = size_effect ? A::size_effect(h, mc) : h;  // se * h
+            const T Ft = A::madd(ktb[s], kse, kteb[s]);
+            T Fr = A::madd(krb[s], kse, kreb[s]);
+            if (pd) Fr = A::madd(pdc[s], A::madd(vxs, sn, vys * cs), Fr);
+            Fx = A::madd(-Ft, cs, A::madd(-Fr, sn, Fx));
+            Fy = A::madd(Ft, sn, A::madd(-Fr, cs, Fy));
+            eng++;
           }
         }
       }
-      p += spt;
-      if (p >= spr) p -= spr;
     }
     Fx = warp_sum(Fx);
     Fy = warp_sum(Fy);
@@ -267,7 +267,14 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     y = ys;
     vxs = vxa;
     vys = vya;
-    if (++pr == spr) pr = 0;
+    // the revolution advances one position: every slot's phase follows
+#pragma unroll
+    for (int s = 0; s < SLOTS; s++) {
+      if (++rph[s] == spt) {
+        rph[s] = 0;
+        if (++cph[s] == N) cph[s] = 0;
+      }
+    }
     if (++phc == spt) {  // once-per-tooth sample (cutting.js:266-268), Float32Array
       phc = 0;
       if (tcount - ts_c0 == lane) {
@@ -279,16 +286,13 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     if (++dcnt == decim) {  // decimated history (cutting.js:288-292), FP64 window sums
       dcnt = 0;
       if (hcount >= h0) {
-        const double hx = (double)(float)((double)x * 1e6), hy = (double)(float)((double)y * 1e6);
+        const float hx = (float)((double)x * 1e6), hy = (float)((double)y * 1e6);
         if (hcount == h0) {
           shx = hx;
           shy = hy;
         }
-        const double dx = hx - shx, dy = hy - shy;
-        sx += dx;
-        sy += dy;
-        sxx = fma(dx, dx, sxx);
-        syy = fma(dy, dy, syy);
+        const double d = (lane & 1) ? (double)hy - (double)shy : (double)hx - (double)shx;
+        acc = (lane & 2) ? fma(d, d, acc) : acc + d;
       }
       hcount++;
     }
@@ -297,6 +301,8 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   // ---- chatterIndex (cutting.js:299-318) in FP64 ----
   res.engaged = (unsigned long long)__reduce_add_sync(kFull, (unsigned)eng);
   res.evals = (unsigned long long)nsteps * (unsigned long long)(N * nz);
+  const double sx = __shfl_sync(kFull, acc, 0), sy = __shfl_sync(kFull, acc, 1),
+               sxx = __shfl_sync(kFull, acc, 2), syy = __shfl_sync(kFull, acc, 3);
   const int n = P->ts_n;
   if (n < 8) {
     res.index = 0.0;
@@ -330,7 +336,7 @@ __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane
 }
 
 // Persistent solve: each warp takes points from the queue and runs timeDomainLimit.
-template <typename T, int SLOTS, int NM>
+template <typename T, int SLOTS, int NM, bool NL>
 __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restrict__ pts,
                                                       const int32_t* __restrict__ order, int n,
                                                       DevOpts o, mcs_result* __restrict__ out,
@@ -361,7 +367,7 @@ __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restr
     } else {
       build_table<T>(P, table, lane);
       auto chatter = [&](double ap, bool& ok) -> bool {
-        const TrialOut t = simulate_trial<T, SLOTS, NM>(P, ap, table, ring, lane);
+        const TrialOut t = simulate_trial<T, SLOTS, NM, NL>(P, ap, table, ring, lane);
         r.trials++;
         r.evals += t.evals;
         r.engaged += t.engaged;
@@ -402,7 +408,7 @@ __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restr
 }
 
 // Batch of independent chatterAt trials (decision replay at given depths).
-template <typename T, int SLOTS, int NM>
+template <typename T, int SLOTS, int NM, bool NL>
 __global__ void __launch_bounds__(kWarp) trials_kernel(const PointParams* __restrict__ pts,
                                                        const TrialItem* __restrict__ items,
                                                        int n, double chatter_idx,
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(kWarp) trials_kernel(const PointParams* __rest
     auto* table = reinterpret_cast<typename Arith<T>::V2*>(smem);
     float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr, sizeof(T) == 8));
     build_table<T>(P, table, lane);
-    const TrialOut t = simulate_trial<T, SLOTS, NM>(P, it.ap, table, ring, lane);
+    const TrialOut t = simulate_trial<T, SLOTS, NM, NL>(P, it.ap, table, ring, lane);
     if (lane == 0) {
       mcs_trial_result r;
       r.index = t.index;
@@ -435,19 +441,21 @@ __global__ void __launch_bounds__(kWarp) trials_kernel(const PointParams* __rest
 }
 
 template <typename T, int SLOTS, int NM>
-void* solve_fn() {
-  return reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM>);
+void* solve_fn(bool nl) {
+  return nl ? reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, true>)
+            : reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, false>);
 }
 template <typename T, int SLOTS, int NM>
-void* trials_fn() {
-  return reinterpret_cast<void*>(&trials_kernel<T, SLOTS, NM>);
+void* trials_fn(bool nl) {
+  return nl ? reinterpret_cast<void*>(&trials_kernel<T, SLOTS, NM, true>)
+            : reinterpret_cast<void*>(&trials_kernel<T, SLOTS, NM, false>);
 }
 
 void* pick(bool solve, const KernelShape& s) {
 #define MCS_PICK(SL, NMV)                                                              \
   if (s.slots == SL && s.modes == NMV)                                                 \
-    return s.fp64 ? (solve ? solve_fn<double, SL, NMV>() : trials_fn<double, SL, NMV>()) \
-                  : (solve ? solve_fn<float, SL, NMV>() : trials_fn<float, SL, NMV>());
+    return s.fp64 ? (solve ? solve_fn<double, SL, NMV>(s.nl) : trials_fn<double, SL, NMV>(s.nl)) \
+                  : (solve ? solve_fn<float, SL, NMV>(s.nl) : trials_fn<float, SL, NMV>(s.nl));
   MCS_PICK(1, 1)
   MCS_PICK(1, 2)
   MCS_PICK(1, 3)
@@ -464,10 +472,11 @@ void* pick(bool solve, const KernelShape& s) {
 
 int set_smem_limits() {
   for (int fp = 0; fp < 2; fp++)
+  for (int nl = 0; nl < 2; nl++)
   for (int sl = 1; sl <= kMaxSlots; sl++)
     for (int nm = 1; nm <= kMaxModes; nm++)
       for (int k = 0; k < 2; k++) {
-        void* f = pick(k == 0, KernelShape{sl, nm, fp});
+        void* f = pick(k == 0, KernelShape{sl, nm, fp, nl});
         cudaError_t e =
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerWarp);
         if (e != cudaSuccess) return (int)e;
