@@ -76,6 +76,23 @@ struct Arith<double> {
   static __device__ __forceinline__ double2 pair(double s, double c) { return make_double2(s, c); }
 };
 
+// Resident warps per SM the register allocation is held to (65536 / (32 * warps)); measured
+// on the sweep, any cap below the natural allocation spills and runs slower (1 = no cap).
+#ifndef MCS_MIN_WARPS_F32
+#define MCS_MIN_WARPS_F32 1
+#endif
+#ifndef MCS_MIN_WARPS_F64
+#define MCS_MIN_WARPS_F64 1
+#endif
+template <typename T>
+struct MinWarps {
+  static constexpr int value = MCS_MIN_WARPS_F32;
+};
+template <>
+struct MinWarps<double> {
+  static constexpr int value = MCS_MIN_WARPS_F64;
+};
+
 struct TrialOut {
   double index, once, amp;
   unsigned long long engaged, evals;
@@ -208,42 +225,52 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   for (int step = 0; step < nsteps; step++) {
     const T xm = x * T(1e3), ym = y * T(1e3);  // tool position [mm]
     T Fx = T(0), Fy = T(0);
+    // rounds u = 0, 1, ...: in each, every lane evaluates, for each of its slots, the tooth
+    // whose window offset is u*spt + r (if in cut); both slots' evaluations are
+    // predicated, not branched, so their dependency chains interleave
+    for (int u = 0; u < N; u++) {
+      int jj[SLOTS];
+      bool act[SLOTS];
+      bool any = false;
 #pragma unroll
-    for (int s = 0; s < SLOTS; s++) {
-      for (int u = 0; u < N; u++) {
-        const int j = u * spt + rph[s];
-        const bool act = j < len[s];
-        if (!__any_sync(kFull, act)) break;  // rounds are monotone: later ones are empty too
+      for (int s = 0; s < SLOTS; s++) {
+        jj[s] = u * spt + rph[s];
+        act[s] = jj[s] < len[s];
+        any |= act[s];
+      }
+      if (!__any_sync(kFull, any)) break;  // rounds are monotone: later ones are empty too
+#pragma unroll
+      for (int s = 0; s < SLOTS; s++) {
         int i = u - cph[s];
         if (i < 0) i += N;
         const T dRi = __shfl_sync(kFull, dRl, i);
-        if (act) {
-          int p = p0[s] + j;  // table position of tooth i at this step
-          if (p >= spr) p -= spr;
-          const typename A::V2 sc = table[p];
-          // phi = p*dphi - lag: rotate the table entry by the slice's helix lag
-          const T sn = A::madd(sc.x, cL[s], -sc.y * sL[s]);
-          const T cs = A::madd(sc.y, cL[s], sc.x * sL[s]);
-          // feed u = [1, 0]: edge normal n = (sin phi, cos phi), tangent t = (cos, -sin)
-          const T rn = A::madd(xm, sn, A::madd(ym, cs, dRi));
-          float* cell = ring + base[s] + j;
-          const T prev = (T)*cell;
-          const T feedH = fzk[s] * sn;
-          T h = (feedH + rn) - prev;
-          if (h <= T(0)) {
-            *cell = (float)(prev - feedH);  // out of cut: the old surface survives
-          } else {
-            *cell = (float)rn;
-            if (h > hmax) h = hmax;  // (a NaN chip stays NaN, as in the reference)
-            const T kse = size_effect ? A::size_effect(h, mc) : h;  // se * h
-            const T Ft = A::madd(ktb[s], kse, kteb[s]);
-            T Fr = A::madd(krb[s], kse, kreb[s]);
-            if (pd) Fr = A::madd(pdc[s], A::madd(vxs, sn, vys * cs), Fr);
-            Fx = A::madd(-Ft, cs, A::madd(-Fr, sn, Fx));
-            Fy = A::madd(Ft, sn, A::madd(-Fr, cs, Fy));
-            eng++;
-          }
-        }
+        // idle lanes (no in-cut tooth this round, or a slice past nz whose ring row does not
+        // exist) read a valid table entry and neither read nor write the ring
+        const int j = act[s] ? jj[s] : 0;
+        int p = p0[s] + j;  // table position of tooth i at this step (p0 < spr, j < spr)
+        if (p >= spr) p -= spr;
+        const typename A::V2 sc = table[p];
+        // phi = p*dphi - lag: rotate the table entry by the slice's helix lag
+        const T sn = A::madd(sc.x, cL[s], -sc.y * sL[s]);
+        const T cs = A::madd(sc.y, cL[s], sc.x * sL[s]);
+        // feed u = [1, 0]: edge normal n = (sin phi, cos phi), tangent t = (cos, -sin)
+        const T rn = A::madd(xm, sn, A::madd(ym, cs, dRi));
+        float* cell = ring + (act[s] ? base[s] + j : 0);
+        const T prev = act[s] ? (T)*cell : T(0);
+        const T feedH = fzk[s] * sn;
+        T h = (feedH + rn) - prev;
+        const bool cut = h > T(0);
+        // out of cut the old surface survives one more feed step (cutting.js:193)
+        if (act[s]) *cell = (float)(cut ? rn : prev - feedH);
+        if (h > hmax) h = hmax;  // (a NaN chip stays NaN, as in the reference)
+        const T kse = size_effect ? A::size_effect(h, mc) : h;  // se * h
+        const T Ft = A::madd(ktb[s], kse, kteb[s]);
+        T Fr = A::madd(krb[s], kse, kreb[s]);
+        if (pd) Fr = A::madd(pdc[s], A::madd(vxs, sn, vys * cs), Fr);
+        const bool on = act[s] && cut;
+        Fx = on ? A::madd(-Ft, cs, A::madd(-Fr, sn, Fx)) : Fx;
+        Fy = on ? A::madd(Ft, sn, A::madd(-Fr, cs, Fy)) : Fy;
+        eng += on ? 1 : 0;
       }
     }
     Fx = warp_sum(Fx);
@@ -337,7 +364,7 @@ __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane
 
 // Persistent solve: each warp takes points from the queue and runs timeDomainLimit.
 template <typename T, int SLOTS, int NM, bool NL>
-__global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restrict__ pts,
+__global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const PointParams* __restrict__ pts,
                                                       const int32_t* __restrict__ order, int n,
                                                       DevOpts o, mcs_result* __restrict__ out,
                                                       unsigned int* __restrict__ queue,
@@ -409,7 +436,7 @@ __global__ void __launch_bounds__(kWarp) solve_kernel(const PointParams* __restr
 
 // Batch of independent chatterAt trials (decision replay at given depths).
 template <typename T, int SLOTS, int NM, bool NL>
-__global__ void __launch_bounds__(kWarp) trials_kernel(const PointParams* __restrict__ pts,
+__global__ void __launch_bounds__(kWarp, MinWarps<T>::value) trials_kernel(const PointParams* __restrict__ pts,
                                                        const TrialItem* __restrict__ items,
                                                        int n, double chatter_idx,
                                                        mcs_trial_result* __restrict__ out,
