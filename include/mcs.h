@@ -254,6 +254,97 @@ int mcs_solve_noalloc(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,
                       const mcs_modal* modals, size_t n_modals, const mcs_point* points,
                       size_t n_points, const mcs_opts* opts, mcs_result* out);
 
+/* ------------------------------------------------------------------ surrogate
+ * A small MLP (20 -> 256 -> 256 -> 256 -> 2, SiLU, BF16 weights and activations with FP32
+ * accumulation) trained on critical depths the time-domain solver itself produces.  For
+ * a point it predicts mu = log critical depth and sigma (a log half-width, Gaussian NLL);
+ * the guided solve verifies the bracket exp(mu -+ hw) with two time-domain trials,
+ * refines it by bisection and falls back to the full bisection when a verification
+ * fails.  No counterpart in the reference: it accelerates timeDomainLimit (stabtd.js:24),
+ * whose plain algorithm remains the judge of every result.
+ */
+#define MCS_FEATURES 20
+
+typedef struct mcs_surrogate mcs_surrogate;
+
+typedef struct {
+  int32_t epochs;      /* passes over the training set (20) */
+  int32_t batch;       /* rows per step (4096) */
+  float lr;            /* Adam step (1e-3) */
+  float beta1, beta2, eps;
+  uint64_t seed;       /* initialisation and shuffling */
+  int32_t warm;        /* nonzero: continue from the current parameters, normalisation and
+                          Adam state instead of a fresh initialisation (0) */
+  int32_t keep_best;   /* nonzero (with a validation set): end with the parameters of the
+                          epoch of lowest validation loss (1) */
+} mcs_train_opts;
+
+typedef struct {
+  float z;             /* bracket half-width hw = clamp(z * sigma, hw_min, hw_max) (log depth) */
+  float hw_min, hw_max;
+  float hw_direct;     /* z * sigma above this: no guess, the full bisection at once */
+  int32_t refine;      /* bisection iterations inside a verified bracket (3) */
+  int32_t pad;
+} mcs_guide_opts;
+
+/* How each point of a guided solve was decided. */
+typedef enum {
+  MCS_PATH_GUIDED = 0,   /* bracket verified and refined */
+  MCS_PATH_FALLBACK = 1, /* a verification failed: full bisection */
+  MCS_PATH_DIRECT = 2,   /* low confidence: full bisection without verification */
+  MCS_PATH_OPEN = 3      /* predicted at or past a_max and stable there */
+} mcs_path;
+
+typedef struct {
+  float mu, sigma;     /* prediction: log critical depth, log half-width */
+  int32_t path;        /* mcs_path */
+  int32_t pad;
+} mcs_guide_info;
+
+void mcs_default_train_opts(mcs_train_opts* o);
+void mcs_default_guide_opts(mcs_guide_opts* o);
+
+/* The 20 raw (unnormalised) input features of each point, out[n * 20]: log R, N,
+ * tan(helix), effective runout, log Ktc, Krc/Ktc, effective mc, log(1 + effective Ci),
+ * arc start, arc end, log fz, log S, log(k zeta) and log fn of the dominant x and y modes
+ * (frf.js:27), sin and cos of 2 pi fn/f_tooth for both dominant modes. */
+int mcs_features(const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+                 size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* opts,
+                 float* out);
+
+/* A surrogate lives on its context's device and is destroyed before the context; destroy
+ * fails with MCS_ERR_STATE while a guided plan still uses it. */
+int mcs_surrogate_create(mcs_ctx* ctx, uint64_t seed, mcs_surrogate** s);
+int mcs_surrogate_destroy(mcs_surrogate* s);
+/* Trains on raw features X[n * 20] and targets y[n] = log critical depth; the feature
+ * normalisation is taken from X.  Per-epoch mean losses go to train_loss / val_loss
+ * (either may be NULL; val set optional). */
+int mcs_surrogate_train(mcs_surrogate* s, const float* X, const float* y, size_t n,
+                        const float* Xv, const float* yv, size_t nv, const mcs_train_opts* o,
+                        float* train_loss, float* val_loss);
+int mcs_surrogate_predict(mcs_surrogate* s, const float* X, size_t n, float* mu, float* sigma);
+/* Mean loss and its gradient for one batch, in the parameter layout (gradient checks). */
+int mcs_surrogate_grad(mcs_surrogate* s, const float* X, const float* y, size_t n, float* loss,
+                       float* grad);
+/* Parameters as one float array: feature mean[20], std[20], then per layer the FP32 master
+ * weights W[K_pad x N_pad] (row-major, K_pad = 32 for the 20 inputs, N_pad = 16 for the 2
+ * outputs, zero padding) and bias[N_pad].  get with out == NULL returns the count. */
+int mcs_surrogate_get_params(mcs_surrogate* s, float* out, size_t* n_floats);
+int mcs_surrogate_set_params(mcs_surrogate* s, const float* in, size_t n_floats);
+
+/* Surrogate-guided timeDomainLimit over a batch; info (may be NULL) gets each point's
+ * prediction and path.  Results are in the mcs_result layout of mcs_solve. */
+int mcs_solve_guided(mcs_ctx* ctx, mcs_surrogate* s, const mcs_setup* setups, size_t n_setups,
+                     const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                     size_t n_points, const mcs_opts* opts, const mcs_guide_opts* g,
+                     mcs_result* out, mcs_guide_info* info);
+/* The same as a device-resident plan (features, inference and solve in one CUDA graph). */
+int mcs_plan_create_guided(mcs_ctx* ctx, mcs_surrogate* s, const mcs_setup* setups,
+                           size_t n_setups, const mcs_modal* modals, size_t n_modals,
+                           const mcs_point* points, size_t n_points, const mcs_opts* opts,
+                           const mcs_guide_opts* g, mcs_plan** plan);
+int mcs_plan_guide_info(mcs_plan* plan, mcs_guide_info* info);
+
 /*
  * Zero-order lobes (sld.js:23-61) read at spindle speeds (alimAt, sld.js:64-76):
  * alim[q * n_rpm + r] for query q at rpm[r]; +inf where no lobe covers the speed.

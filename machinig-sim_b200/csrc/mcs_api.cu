@@ -19,10 +19,10 @@
 using namespace mcs;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
-int fail(int code, const char* fmt, ...) {
+int mcs::fail(int code, const char* fmt, ...) {
   char buf[512];
   va_list ap;
   va_start(ap, fmt);
@@ -31,6 +31,8 @@ int fail(int code, const char* fmt, ...) {
   g_last_error = buf;
   return code;
 }
+
+namespace {
 
 #define MCS_CUDA(call)                                                                    \
   do {                                                                                    \
@@ -242,6 +244,47 @@ int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const m
 
 int slots_for(int nz) { return nz <= kWarp ? 1 : 2; }
 
+// The surrogate's 20 raw input features of a point (mcs_features in include/mcs.h).
+void point_features(const mcs_setup& st, const mcs_modal& md, double S_in, const mcs_opts& o,
+                    float* f) {
+  const mcs_tool& t = st.tool;
+  const mcs_material& m = st.mat;
+  const int nx = md.nx, ny = md.ny > 0 ? md.ny : md.nx;
+  const mcs_mode* xm = md.x;
+  const mcs_mode* ym = md.ny > 0 ? md.y : md.x;
+  // dominant mode: the lowest k * zeta, the first of equals (frf.js:27)
+  auto dominant = [](const mcs_mode* ms, int n) {
+    int a = 0;
+    for (int i = 1; i < n; i++)
+      if (ms[i].k * ms[i].zeta < ms[a].k * ms[a].zeta) a = i;
+    return ms[a];
+  };
+  const mcs_mode dx = dominant(xm, nx), dy = dominant(ym, ny);
+  const double S = std::max(100.0, S_in);
+  const double ft = S * t.N / 60.0;  // tooth-passing frequency [Hz]
+  const double two_pi = 2 * kPi;
+  f[0] = (float)std::log(t.R);
+  f[1] = (float)t.N;
+  f[2] = (float)std::tan(t.helix_deg * kPi / 180);
+  f[3] = (float)(o.honor_runout ? t.runout : 0.0);
+  f[4] = (float)std::log(std::max(m.Ktc, 1e-9));
+  f[5] = (float)(m.Krc / std::max(m.Ktc, 1e-9));
+  f[6] = (float)(o.nonlinear ? m.mc : 0.0);
+  f[7] = (float)std::log1p(o.nonlinear ? m.Ci : 0.0);
+  f[8] = (float)st.arc_st;
+  f[9] = (float)st.arc_ex;
+  f[10] = (float)std::log(st.fz);
+  f[11] = (float)std::log(S);
+  f[12] = (float)std::log(dx.k * std::max(dx.zeta, 1e-6));
+  f[13] = (float)std::log(dx.fn);
+  f[14] = (float)std::log(dy.k * std::max(dy.zeta, 1e-6));
+  f[15] = (float)std::log(dy.fn);
+  f[16] = (float)std::sin(two_pi * dx.fn / ft);
+  f[17] = (float)std::cos(two_pi * dx.fn / ft);
+  f[18] = (float)std::sin(two_pi * dy.fn / ft);
+  f[19] = (float)std::cos(two_pi * dy.fn / ft);
+}
+
 // ------------------------------------------------------------------ device buffers
 struct DevBuf {
   void* p = nullptr;
@@ -292,10 +335,17 @@ struct mcs_ctx {
   size_t pinned_cap = 0;
 };
 
+int mcs::ctx_device(mcs_ctx* c) { return c->device; }
+cudaStream_t mcs::ctx_stream(mcs_ctx* c) { return c->stream; }
+
 struct mcs_plan {
   mcs_ctx* ctx = nullptr;
   size_t n = 0;
   bool trials = false;
+  // surrogate guidance (guided plans)
+  mcs_surrogate* sur = nullptr;
+  mcs_guide_opts gopts{};
+  DevBuf feat, gmu, gsigma, guide, ginfo;
   std::vector<Bucket> buckets;
   DevBuf params, order, results, queues, items;
   cudaGraph_t graph = nullptr;
@@ -394,6 +444,19 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
   MCS_CUDA(cudaMemsetAsync(pl->queues.p, 0, sizeof(unsigned int) * std::max(1, nb), s0));
   if (progress) MCS_CUDA(cudaMemsetAsync(progress, 0, sizeof(unsigned int), s0));
   if (nb == 0) return MCS_OK;
+  GuideArgs ga;
+  if (pl->sur) {
+    const int rc = surrogate_predict_device(pl->sur, static_cast<const float*>(pl->feat.p),
+                                            (long)pl->n, static_cast<float*>(pl->gmu.p),
+                                            static_cast<float*>(pl->gsigma.p),
+                                            static_cast<float2*>(pl->guide.p), &pl->gopts, s0);
+    if (rc) return rc;
+    ga.guide = static_cast<const float2*>(pl->guide.p);
+    ga.sigma = static_cast<const float*>(pl->gsigma.p);
+    ga.info = static_cast<mcs_guide_info*>(pl->ginfo.p);
+    ga.hw_min = pl->gopts.hw_min;
+    ga.refine = pl->gopts.refine;
+  }
   MCS_CUDA(cudaEventRecord(ctx->fork, s0));
   for (int b = 0; b < nb; b++) {
     const Bucket& bk = pl->buckets[b];
@@ -411,7 +474,7 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
       rc = launch_solve(bk.shape, bk.grid, bk.smem, sb,
                         static_cast<const PointParams*>(pl->params.p), order, bk.count,
                         dev_opts(o), static_cast<mcs_result*>(pl->results.p), q, cancel,
-                        progress);
+                        progress, ga);
     if (rc != 0)
       return fail(MCS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString((cudaError_t)rc));
     if (sb != s0) {
@@ -431,6 +494,12 @@ void plan_free(mcs_plan* pl) {
   pl->results.release();
   pl->queues.release();
   pl->items.release();
+  pl->feat.release();
+  pl->gmu.release();
+  pl->gsigma.release();
+  pl->guide.release();
+  pl->ginfo.release();
+  if (pl->sur) surrogate_hold(pl->sur, -1);
   delete pl;
 }
 
@@ -464,9 +533,13 @@ int upload2(mcs_ctx* ctx, cudaStream_t stream, void* d1, const void* h1, size_t 
 // Validates, prepares and uploads a solve batch; optionally captures it in a graph.
 int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
                size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* o,
-               bool capture, cudaStream_t stream, mcs_plan** out) {
+               bool capture, cudaStream_t stream, mcs_plan** out,
+               mcs_surrogate* sur = nullptr, const mcs_guide_opts* g = nullptr) {
   int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
   if (rc) return rc;
+  if (sur && (!g || !(g->z > 0) || !(g->hw_min > 0) || !(g->hw_max >= g->hw_min) ||
+              !(g->hw_direct > 0) || g->refine < 0 || g->refine > 30))
+    return fail(MCS_ERR_ARG, "guide options out of range");
   std::vector<PointParams> pp(n_points);
   std::vector<int> smem(n_points), slots(n_points), modes(n_points), nls(n_points);
   std::vector<double> cost(n_points);
@@ -511,6 +584,31 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   for (const Bucket& b : pl->buckets) {
     pl->max_modes = std::max(pl->max_modes, b.shape.modes);
     pl->max_slots = std::max(pl->max_slots, b.shape.slots);
+  }
+  if (sur && n_points) {
+    pl->sur = sur;
+    surrogate_hold(sur, +1);
+    pl->gopts = *g;
+    std::vector<float> f(n_points * MCS_FEATURES);
+    for (size_t i = 0; i < n_points; i++)
+      point_features(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,
+                     &f[i * MCS_FEATURES]);
+    if ((rc = pl->feat.ensure(sizeof(float) * f.size())) ||
+        (rc = pl->gmu.ensure(sizeof(float) * n_points)) ||
+        (rc = pl->gsigma.ensure(sizeof(float) * n_points)) ||
+        (rc = pl->guide.ensure(sizeof(float2) * n_points)) ||
+        (rc = pl->ginfo.ensure(sizeof(mcs_guide_info) * n_points)) ||
+        (rc = surrogate_reserve(sur))) {
+      plan_free(pl);
+      return rc;
+    }
+    cudaError_t e = cudaMemcpyAsync(pl->feat.p, f.data(), sizeof(float) * f.size(),
+                                    cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+      plan_free(pl);
+      return fail(MCS_ERR_CUDA, "feature upload failed: %s", cudaGetErrorString(e));
+    }
   }
   if (capture) {
     cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
@@ -876,6 +974,73 @@ void mcs_job_free(mcs_job* jb) {
   cudaEventDestroy(jb->done);
   cudaStreamDestroy(jb->stream);
   delete jb;
+}
+
+int mcs_features(const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+                 size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* o,
+                 float* out) {
+  if (n_points && !out) return fail(MCS_ERR_ARG, "out is NULL");
+  int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
+  if (rc) return rc;
+  for (size_t i = 0; i < n_points; i++)
+    point_features(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,
+                   out + i * MCS_FEATURES);
+  return MCS_OK;
+}
+
+int mcs_solve_guided(mcs_ctx* c, mcs_surrogate* sur, const mcs_setup* setups, size_t n_setups,
+                     const mcs_modal* modals, size_t n_modals, const mcs_point* points,
+                     size_t n_points, const mcs_opts* opts, const mcs_guide_opts* g,
+                     mcs_result* out, mcs_guide_info* info) {
+  if (!c || !sur) return fail(MCS_ERR_ARG, "NULL ctx or surrogate");
+  if (surrogate_ctx(sur) != c) return fail(MCS_ERR_ARG, "surrogate belongs to another context");
+  if (n_points && !out) return fail(MCS_ERR_ARG, "out is NULL");
+  std::lock_guard<std::mutex> lk(c->mu);
+  std::lock_guard<std::mutex> slk(surrogate_mutex(sur));
+  MCS_CUDA(cudaSetDevice(c->device));
+  mcs_plan* pl = nullptr;
+  int rc = build_plan(c, setups, n_setups, modals, n_modals, points, n_points, opts, false,
+                      c->stream, &pl, sur, g);
+  if (rc) return rc;
+  rc = enqueue(pl, c->stream, opts, nullptr, nullptr, opts->chatter_idx);
+  if (!rc && n_points) {
+    cudaError_t e = cudaMemcpyAsync(out, pl->results.p, sizeof(mcs_result) * n_points,
+                                    cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && info)
+      e = cudaMemcpyAsync(info, pl->ginfo.p, sizeof(mcs_guide_info) * n_points,
+                          cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "result copy failed: %s", cudaGetErrorString(e));
+  }
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "guided solve failed: %s", cudaGetErrorString(e));
+  plan_free(pl);
+  return rc;
+}
+
+int mcs_plan_create_guided(mcs_ctx* c, mcs_surrogate* sur, const mcs_setup* setups,
+                           size_t n_setups, const mcs_modal* modals, size_t n_modals,
+                           const mcs_point* points, size_t n_points, const mcs_opts* opts,
+                           const mcs_guide_opts* g, mcs_plan** plan) {
+  if (!c || !sur || !plan) return fail(MCS_ERR_ARG, "NULL ctx, surrogate or plan pointer");
+  if (surrogate_ctx(sur) != c) return fail(MCS_ERR_ARG, "surrogate belongs to another context");
+  std::lock_guard<std::mutex> lk(c->mu);
+  std::lock_guard<std::mutex> slk(surrogate_mutex(sur));
+  MCS_CUDA(cudaSetDevice(c->device));
+  return build_plan(c, setups, n_setups, modals, n_modals, points, n_points, opts, true,
+                    c->stream, plan, sur, g);
+}
+
+int mcs_plan_guide_info(mcs_plan* pl, mcs_guide_info* info) {
+  if (!pl || (!info && pl->n)) return fail(MCS_ERR_ARG, "NULL plan or output");
+  if (!pl->sur) return fail(MCS_ERR_STATE, "the plan is not guided");
+  if (!pl->executed) return fail(MCS_ERR_STATE, "plan was never executed");
+  std::lock_guard<std::mutex> lk(pl->ctx->mu);
+  MCS_CUDA(cudaSetDevice(pl->ctx->device));
+  if (pl->n)
+    MCS_CUDA(cudaMemcpyAsync(info, pl->ginfo.p, sizeof(mcs_guide_info) * pl->n,
+                             cudaMemcpyDeviceToHost, pl->ctx->stream));
+  MCS_CUDA(cudaStreamSynchronize(pl->ctx->stream));
+  return MCS_OK;
 }
 
 int mcs_lobes_alim(mcs_ctx* c, const mcs_modal* modals, size_t n_modals,

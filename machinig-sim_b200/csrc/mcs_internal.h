@@ -6,7 +6,24 @@
 
 #include "../../include/mcs.h"
 
+#include <cuda_runtime.h>
+
+#include <mutex>
+
 namespace mcs {
+
+// Records a message for mcs_last_error() (per thread) and returns code.
+int fail(int code, const char* fmt, ...);
+
+#define MCS_CUDA_RET(call)                                                                \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return ::mcs::fail(MCS_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+  } while (0)
+
+int ctx_device(mcs_ctx* ctx);
+cudaStream_t ctx_stream(mcs_ctx* ctx);
 
 constexpr int kMaxTeeth = MCS_MAX_TEETH;
 constexpr int kMaxModes = MCS_MAX_MODES;
@@ -61,6 +78,15 @@ struct DevOpts {
   int32_t iters, pad;
 };
 
+// Surrogate guidance of the solve kernel (all NULL: the plain algorithm).
+struct GuideArgs {
+  const float2* guide = nullptr;  // per point (mu, hw) of the log depth; hw < 0: no guess
+  const float* sigma = nullptr;   // per point predicted sigma (reported only)
+  mcs_guide_info* info = nullptr; // per point path taken
+  float hw_min = 0.f;             // half-width the refinement count is calibrated on
+  int refine = 0;                 // halvings of a hw_min bracket
+};
+
 // One chatterAt trial of the batch kernel.
 struct TrialItem {
   int32_t point;   // index into the PointParams array
@@ -80,13 +106,22 @@ struct KernelShape {
 int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                  const PointParams* pts, const int32_t* order, int n, DevOpts opts,
                  mcs_result* out, unsigned int* queue, const volatile int* cancel,
-                 unsigned int* progress);
+                 unsigned int* progress, const GuideArgs& guide = GuideArgs());
 int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                   const PointParams* pts, const TrialItem* items, int n, double chatter_idx,
                   mcs_trial_result* out, unsigned int* queue);
 int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm);
 int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm);
 int set_smem_limits();
+// surrogate (mcs_surrogate.cu)
+int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d_mu,
+                             float* d_sigma, float2* d_guide, const mcs_guide_opts* g,
+                             cudaStream_t st);
+int surrogate_reserve(mcs_surrogate* s);
+mcs_ctx* surrogate_ctx(mcs_surrogate* s);
+std::mutex& surrogate_mutex(mcs_surrogate* s);
+// guided plans that hold the surrogate (it cannot be destroyed while any do)
+void surrogate_hold(mcs_surrogate* s, int delta);
 int launch_lobes(cudaStream_t stream, const mcs_modal* modals, const mcs_lobe_query* qs, int n_q,
                  const double* rpm, int n_rpm, double* out);
 

@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
                                                       DevOpts o, mcs_result* __restrict__ out,
                                                       unsigned int* __restrict__ queue,
                                                       const volatile int* cancel,
-                                                      unsigned int* progress) {
+                                                      unsigned int* progress, GuideArgs g) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x;
   for (;;) {
@@ -393,37 +393,100 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
       r.status = MCS_ERR_CANCELLED;
     } else {
       build_table<T>(P, table, lane);
-      auto chatter = [&](double ap, bool& ok) -> bool {
+      auto chatter = [&](double ap) -> bool {
         const TrialOut t = simulate_trial<T, SLOTS, NM, NL>(P, ap, table, ring, lane);
         r.trials++;
         r.evals += t.evals;
         r.engaged += t.engaged;
         if (t.status != MCS_OK) r.status = t.status;
-        ok = t.status == MCS_OK;
         return t.index > o.chatter_idx;
       };
-      bool ok = true;
-      if (!chatter(o.a_max, ok)) {
-        r.alim = o.a_max;
-        r.lo = o.a_max;
-        r.hi = INFINITY;
-        r.open = 1;
-      } else {
-        double lo = o.a_min, hi = o.a_max;
-        for (int it = 0; it < o.iters; it++) {
-          if (read_cancel(cancel, lane)) {
-            r.status = MCS_ERR_CANCELLED;
-            break;
+      bool done = false;
+      bool top_chatters = false;  // the first plain trial, chatter(a_max), already ran
+      int path = MCS_PATH_DIRECT;
+      if (g.guide != nullptr && g.guide[pi].y >= 0.f) {
+        // surrogate-guided: the plain first trial at a_max (stabtd.js:25) runs as it does
+        // without a guide, so open points come out exactly as in the plain method; then
+        // the bracket exp(mu -+ hw), kept inside [a_min, a_max], must be stable at its
+        // lower and chatter at its upper end and is refined by the same geometric
+        // bisection.  A failed verification falls back to the full bisection.
+        const float2 gd = g.guide[pi];
+        if (!chatter(o.a_max)) {
+          r.alim = o.a_max;
+          r.lo = o.a_max;
+          r.hi = INFINITY;
+          r.open = 1;
+          path = MCS_PATH_OPEN;
+          done = true;
+        } else {
+          top_chatters = true;
+          const double hw = (double)gd.y;
+          double lo = exp((double)gd.x - hw), hi = exp((double)gd.x + hw);
+          if (lo < o.a_min) {  // shift up to start at a_min
+            lo = o.a_min;
+            hi = fmin(fmax(hi, o.a_min * exp(2.0 * hw)), o.a_max);
           }
-          const double m = sqrt(lo * hi);
-          if (chatter(m, ok))
-            hi = m;
-          else
-            lo = m;
+          if (hi > o.a_max) {  // shift down to end at a_max
+            hi = o.a_max;
+            lo = fmax(fmin(lo, o.a_max * exp(-2.0 * hw)), o.a_min);
+          }
+          bool ok = lo < hi;
+          if (ok && hi < o.a_max) ok = chatter(hi);   // a_max is known to chatter
+          if (ok && lo > o.a_min) ok = !chatter(lo);  // a_min is taken as stable, as plain does
+          if (ok) {
+            // enough halvings that the final bracket is no wider than a hw_min bracket's
+            // after `refine` halvings
+            int iters = g.refine;
+            for (double w = log(hi / lo) * 0.5; w > 1.0000001 * (double)g.hw_min; w *= 0.5)
+              iters++;
+            for (int it = 0; it < iters; it++) {
+              const double m = sqrt(lo * hi);
+              if (chatter(m))
+                hi = m;
+              else
+                lo = m;
+            }
+            r.alim = sqrt(lo * hi);
+            r.lo = lo;
+            r.hi = hi;
+            path = MCS_PATH_GUIDED;
+            done = true;
+          } else {
+            path = MCS_PATH_FALLBACK;
+          }
         }
-        r.alim = sqrt(lo * hi);
-        r.lo = lo;
-        r.hi = hi;
+      }
+      if (!done) {  // the reference's algorithm (stabtd.js:24-32)
+        if (!top_chatters && !chatter(o.a_max)) {
+          r.alim = o.a_max;
+          r.lo = o.a_max;
+          r.hi = INFINITY;
+          r.open = 1;
+        } else {
+          double lo = o.a_min, hi = o.a_max;
+          for (int it = 0; it < o.iters; it++) {
+            if (read_cancel(cancel, lane)) {
+              r.status = MCS_ERR_CANCELLED;
+              break;
+            }
+            const double m = sqrt(lo * hi);
+            if (chatter(m))
+              hi = m;
+            else
+              lo = m;
+          }
+          r.alim = sqrt(lo * hi);
+          r.lo = lo;
+          r.hi = hi;
+        }
+      }
+      if (g.info != nullptr && lane == 0) {
+        mcs_guide_info gi;
+        gi.mu = g.guide ? g.guide[pi].x : 0.f;
+        gi.sigma = g.sigma ? g.sigma[pi] : 0.f;
+        gi.path = path;
+        gi.pad = 0;
+        g.info[pi] = gi;
       }
     }
     if (lane == 0) {
@@ -528,10 +591,11 @@ int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm) {
 int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                  const PointParams* pts, const int32_t* order, int n, DevOpts opts,
                  mcs_result* out, unsigned int* queue, const volatile int* cancel,
-                 unsigned int* progress) {
+                 unsigned int* progress, const GuideArgs& guide) {
   void* f = pick(true, shape);
   if (!f) return (int)cudaErrorInvalidValue;
-  void* args[] = {&pts, &order, &n, &opts, &out, &queue, &cancel, &progress};
+  GuideArgs g = guide;
+  void* args[] = {&pts, &order, &n, &opts, &out, &queue, &cancel, &progress, &g};
   return (int)cudaLaunchKernel(f, dim3(grid), dim3(kWarp), args, (size_t)smem, stream);
 }
 

@@ -1,0 +1,769 @@
+// The learned surrogate: an MLP 20 -> 256 -> 256 -> 256 -> 2 (SiLU) trained with a
+// Gaussian negative log-likelihood on log critical depths the time-domain solver
+// produced.  Weights and activations are BF16, every product accumulates in FP32
+// (mma.sync m16n8k16), the Adam state and master weights are FP32.
+//
+// Layers are padded to tensor-core shapes: the 20 inputs to 32, the 2 outputs to 16;
+// padded weights start at zero and get zero gradients, so they stay zero.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "mcs_internal.h"
+
+namespace mcs {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kIn = MCS_FEATURES;
+constexpr int kInPad = 32;
+constexpr int kHid = 256;
+constexpr int kOutPad = 16;
+constexpr int kLayers = 4;
+constexpr int kK[kLayers] = {kInPad, kHid, kHid, kHid};
+constexpr int kN[kLayers] = {kHid, kHid, kHid, kOutPad};
+constexpr float kSMin = -7.f, kSMax = 5.f;  // range of the predicted log sigma
+
+// offsets of the parameter blob (floats)
+struct Layout {
+  size_t mean = 0, stdv = kIn, W[kLayers], b[kLayers], total;
+  Layout() {
+    size_t o = 2 * kIn;
+    for (int l = 0; l < kLayers; l++) {
+      W[l] = o;
+      o += (size_t)kK[l] * kN[l];
+      b[l] = o;
+      o += kN[l];
+    }
+    total = o;
+  }
+};
+const Layout kLay;
+
+// ---------------------------------------------------------------- kernels
+__device__ __forceinline__ uint16_t bf_bits(const bf16* p, long i, bool ok) {
+  return ok ? __bfloat16_as_ushort(p[i]) : (uint16_t)0;
+}
+__device__ __forceinline__ uint32_t pack2(uint16_t lo, uint16_t hi) {
+  return (uint32_t)lo | ((uint32_t)hi << 16);
+}
+
+// C[M x N] (+)= A[M x K] * B[K x N]; A(m, k) = A[m*sAm + k*sAk], B(k, n) = B[k*sBk + n*sBn]
+// (strides express the transposes of the backward pass).  4 warps per block, each a
+// 32 x 32 tile as 2 x 4 mma.sync.m16n8k16 (BF16 in, FP32 accumulate).
+__global__ void __launch_bounds__(128) gemm_bf16(const bf16* __restrict__ A, long sAm, long sAk,
+                                                 const bf16* __restrict__ B, long sBk, long sBn,
+                                                 float* __restrict__ C, long ldc, int M, int N,
+                                                 int K, int accumulate) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = blockIdx.y * 64 + (warp & 1) * 32;
+  const int n0 = blockIdx.x * 64 + (warp >> 1) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    uint32_t a[2][4], b[4][2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      const int r0 = m0 + 16 * i + g, r1 = r0 + 8;
+      const int c0 = k0 + 2 * t, c1 = c0 + 8;
+      const bool v00 = r0 < M && c0 < K, v01 = r0 < M && c0 + 1 < K;
+      const bool v10 = r1 < M && c0 < K, v11 = r1 < M && c0 + 1 < K;
+      const bool w00 = r0 < M && c1 < K, w01 = r0 < M && c1 + 1 < K;
+      const bool w10 = r1 < M && c1 < K, w11 = r1 < M && c1 + 1 < K;
+      a[i][0] = pack2(bf_bits(A, r0 * sAm + c0 * sAk, v00), bf_bits(A, r0 * sAm + (c0 + 1) * sAk, v01));
+      a[i][1] = pack2(bf_bits(A, r1 * sAm + c0 * sAk, v10), bf_bits(A, r1 * sAm + (c0 + 1) * sAk, v11));
+      a[i][2] = pack2(bf_bits(A, r0 * sAm + c1 * sAk, w00), bf_bits(A, r0 * sAm + (c1 + 1) * sAk, w01));
+      a[i][3] = pack2(bf_bits(A, r1 * sAm + c1 * sAk, w10), bf_bits(A, r1 * sAm + (c1 + 1) * sAk, w11));
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int n = n0 + 8 * j + g;
+      const int k = k0 + 2 * t;
+      const bool vn = n < N;
+      b[j][0] = pack2(bf_bits(B, k * sBk + n * sBn, vn && k < K),
+                      bf_bits(B, (k + 1) * sBk + n * sBn, vn && k + 1 < K));
+      b[j][1] = pack2(bf_bits(B, (k + 8) * sBk + n * sBn, vn && k + 8 < K),
+                      bf_bits(B, (k + 9) * sBk + n * sBn, vn && k + 9 < K));
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
+            "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+            : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]),
+              "r"(b[j][1]));
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int r = m0 + 16 * i + g + (e >= 2 ? 8 : 0);
+        const int c = n0 + 8 * j + 2 * t + (e & 1);
+        if (r < M && c < N) {
+          float* o = C + (long)r * ldc + c;
+          *o = accumulate ? *o + acc[i][j][e] : acc[i][j][e];
+        }
+      }
+}
+
+__device__ __forceinline__ float sigmoid(float z) { return 1.f / (1.f + __expf(-z)); }
+
+// z = C + bias (kept for the backward pass); out = BF16(silu(z)) or, for the last layer,
+// the FP32 z itself
+__global__ void bias_act(const float* __restrict__ C, const float* __restrict__ bias, int M,
+                         int N, float* __restrict__ z, bf16* __restrict__ out, int act) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)M * N) return;
+  const float v = C[i] + bias[i % N];
+  if (z) z[i] = v;
+  if (out) out[i] = __float2bfloat16(act ? v * sigmoid(v) : v);
+}
+
+// Gaussian NLL of y under N(mu, exp(s)^2) with (mu, s) = out[:, 0:2]; writes d loss / d out
+// (divided by the batch) in FP32 and BF16 and adds the summed loss to *loss.
+__global__ void nll_loss(const float* __restrict__ out, const float* __restrict__ y, int B,
+                         float* __restrict__ dout, bf16* __restrict__ doutb,
+                         float* __restrict__ loss) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.f;
+  if (b < B) {
+    const float mu = out[(long)b * kOutPad], s_raw = out[(long)b * kOutPad + 1];
+    const float s = fminf(fmaxf(s_raw, kSMin), kSMax);
+    const float r = y[b] - mu, iv = __expf(-2.f * s);
+    l = s + 0.5f * r * r * iv;
+    const float inB = 1.f / (float)B;
+    const float dmu = -r * iv * inB;
+    const float ds = (s_raw > kSMin && s_raw < kSMax) ? (1.f - r * r * iv) * inB : 0.f;
+    for (int c = 0; c < kOutPad; c++) {
+      const float d = c == 0 ? dmu : (c == 1 ? ds : 0.f);
+      dout[(long)b * kOutPad + c] = d;
+      doutb[(long)b * kOutPad + c] = __float2bfloat16(d);
+    }
+  }
+  // warp, then block reduction of the loss
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+  __shared__ float part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = l;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float s = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += part[w];
+    atomicAdd(loss, s);
+  }
+}
+
+// dz = dh * silu'(z) in FP32 and BF16
+__global__ void silu_back(const float* __restrict__ dh, const float* __restrict__ z, long n,
+                          float* __restrict__ dz, bf16* __restrict__ dzb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v = z[i], sg = sigmoid(v);
+  const float d = dh[i] * sg * (1.f + v * (1.f - sg));
+  dz[i] = d;
+  dzb[i] = __float2bfloat16(d);
+}
+
+// db[c] = sum over rows of dz[:, c]
+__global__ void col_sum(const float* __restrict__ dz, int M, int N, float* __restrict__ db) {
+  const int c = blockIdx.x;
+  float s = 0.f;
+  for (int r = threadIdx.x; r < M; r += blockDim.x) s += dz[(long)r * N + c];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ float part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+    db[c] = t;
+  }
+}
+
+// Adam on the trainable part of the parameter blob (bias-corrected)
+__global__ void adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                     const float* __restrict__ g, long n, float lr, float b1, float b2, float eps,
+                     float c1, float c2) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void to_bf16(const float* __restrict__ x, long n, bf16* __restrict__ y) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = __float2bfloat16(x[i]);
+}
+
+// rows idx[off + b] (or off + b without idx) of the raw features, normalised, BF16, padded
+__global__ void gather_rows(const float* __restrict__ X, const int32_t* __restrict__ idx,
+                            long off, int B, long n, const float* __restrict__ mean,
+                            const float* __restrict__ stdv, const float* __restrict__ y,
+                            bf16* __restrict__ xb, float* __restrict__ yb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)B * kInPad) return;
+  const int b = (int)(i / kInPad), c = (int)(i % kInPad);
+  const long row = idx ? (long)idx[off + b] : off + b;
+  float v = 0.f;
+  if (c < kIn && row < n) v = (X[row * kIn + c] - mean[c]) / stdv[c];
+  xb[i] = __float2bfloat16(v);
+  if (c == 0 && yb) yb[b] = row < n ? y[row] : 0.f;
+}
+
+// prediction -> (mu, sigma), and the guide (mu, hw) of the guided solve (hw < 0: direct)
+__global__ void predict_out(const float* __restrict__ out, int n, float* __restrict__ mu,
+                            float* __restrict__ sigma, float2* __restrict__ guide, float z,
+                            float hw_min, float hw_max, float hw_direct) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float m = out[(long)b * kOutPad];
+  const float s = expf(fminf(fmaxf(out[(long)b * kOutPad + 1], kSMin), kSMax));
+  if (mu) mu[b] = m;
+  if (sigma) sigma[b] = s;
+  if (guide) {
+    const float w = z * s;
+    guide[b] = make_float2(m, w > hw_direct ? -1.f : fminf(fmaxf(w, hw_min), hw_max));
+  }
+}
+
+inline int blocks(long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+}  // namespace mcs
+
+using namespace mcs;
+
+namespace mcs {
+namespace {
+// Activations (and gradients) of one batch of up to `cap` rows.
+struct Acts {
+  int cap = 0;
+  bf16* xb = nullptr;
+  float* yb = nullptr;
+  float* z[kLayers] = {};
+  bf16* a[kLayers] = {};
+  float* C = nullptr;   // GEMM output
+  float* dz = nullptr;  // FP32 d loss / d z
+  bf16* dzb = nullptr;
+  float* dh = nullptr;
+};
+constexpr int kInferRows = 16384;  // inference chunk; its buffers are never reallocated
+}  // namespace
+}  // namespace mcs
+
+struct mcs_surrogate {
+  mcs_ctx* ctx = nullptr;
+  uint64_t seed = 0;
+  bool trained = false;
+  float* params = nullptr;  // FP32 blob on the device
+  float* grad = nullptr;
+  float* m = nullptr;
+  float* v = nullptr;
+  bf16* Wb[kLayers] = {};
+  long step = 0;
+  Acts inf;  // inference (captured plans keep pointers into it)
+  Acts tr;   // training and gradients
+  float* loss = nullptr;
+  std::atomic<int> plans{0};  // guided plans holding this surrogate
+  std::mutex mu;
+};
+
+namespace mcs {
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+  *p = nullptr;
+  const cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? MCS_ERR_NOMEM : MCS_ERR_CUDA,
+                "cudaMalloc failed: %s", cudaGetErrorString(e));
+  }
+  return MCS_OK;
+}
+
+void free_acts(Acts& s) {
+  cudaFree(s.xb);
+  cudaFree(s.yb);
+  for (int l = 0; l < kLayers; l++) {
+    cudaFree(s.z[l]);
+    cudaFree(s.a[l]);
+  }
+  cudaFree(s.C);
+  cudaFree(s.dz);
+  cudaFree(s.dzb);
+  cudaFree(s.dh);
+  s = Acts();
+}
+
+int ensure_acts(Acts& s, int rows) {
+  if (rows <= s.cap) return MCS_OK;
+  free_acts(s);
+  int rc;
+  const size_t r = (size_t)rows;
+  if ((rc = dalloc(&s.xb, r * kInPad)) || (rc = dalloc(&s.yb, r)) ||
+      (rc = dalloc(&s.C, r * kHid)) || (rc = dalloc(&s.dz, r * kHid)) ||
+      (rc = dalloc(&s.dzb, r * kHid)) || (rc = dalloc(&s.dh, r * kHid))) {
+    free_acts(s);
+    return rc;
+  }
+  for (int l = 0; l < kLayers; l++)
+    if ((rc = dalloc(&s.z[l], r * kN[l])) || (rc = dalloc(&s.a[l], r * kN[l]))) {
+      free_acts(s);
+      return rc;
+    }
+  s.cap = rows;
+  return MCS_OK;
+}
+
+// xorshift-free reproducible normal draws for the initialisation (SplitMix64 + Box-Muller)
+struct Rng {
+  uint64_t s;
+  uint64_t next() {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+  }
+  double uniform() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+void init_host(std::vector<float>& p, uint64_t seed) {
+  p.assign(kLay.total, 0.f);
+  for (int c = 0; c < kIn; c++) p[kLay.stdv + c] = 1.f;
+  Rng rng{seed ^ 0xC0FFEEULL};
+  const int fan_in[kLayers] = {kIn, kHid, kHid, kHid};
+  for (int l = 0; l < kLayers; l++) {
+    const int K = kK[l], N = kN[l];
+    const int kreal = l == 0 ? kIn : K, nreal = l == kLayers - 1 ? 2 : N;
+    const double lim = std::sqrt(6.0 / fan_in[l]) * (l == kLayers - 1 ? 0.1 : 1.0);
+    for (int k = 0; k < kreal; k++)
+      for (int n = 0; n < nreal; n++)
+        p[kLay.W[l] + (size_t)k * N + n] = (float)((2 * rng.uniform() - 1) * lim);
+  }
+}
+
+int upload_params(mcs_surrogate* s, const float* host) {
+  MCS_CUDA_RET(cudaMemcpy(s->params, host, kLay.total * sizeof(float), cudaMemcpyHostToDevice));
+  MCS_CUDA_RET(cudaMemset(s->m, 0, kLay.total * sizeof(float)));
+  MCS_CUDA_RET(cudaMemset(s->v, 0, kLay.total * sizeof(float)));
+  s->step = 0;
+  return MCS_OK;
+}
+
+int cast_weights(mcs_surrogate* s, cudaStream_t st) {
+  for (int l = 0; l < kLayers; l++) {
+    const long n = (long)kK[l] * kN[l];
+    to_bf16<<<blocks(n, 256), 256, 0, st>>>(s->params + kLay.W[l], n, s->Wb[l]);
+  }
+  MCS_CUDA_RET(cudaGetLastError());
+  return MCS_OK;
+}
+
+void gemm(cudaStream_t st, const bf16* A, long sAm, long sAk, const bf16* B, long sBk, long sBn,
+          float* C, long ldc, int M, int N, int K, bool accumulate) {
+  const dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
+  gemm_bf16<<<grid, 128, 0, st>>>(A, sAm, sAk, B, sBk, sBn, C, ldc, M, N, K, accumulate ? 1 : 0);
+}
+
+// forward of rows already in A.xb; final FP32 output in A.z[3]
+void forward(mcs_surrogate* s, Acts& A, int rows, cudaStream_t st) {
+  const bf16* x = A.xb;
+  for (int l = 0; l < kLayers; l++) {
+    const int K = kK[l], N = kN[l];
+    gemm(st, x, K, 1, s->Wb[l], N, 1, A.C, N, rows, N, K, false);
+    const long n = (long)rows * N;
+    const bool last = l == kLayers - 1;
+    bias_act<<<blocks(n, 256), 256, 0, st>>>(A.C, s->params + kLay.b[l], rows, N, A.z[l],
+                                             last ? nullptr : A.a[l], last ? 0 : 1);
+    x = A.a[l];
+  }
+}
+
+// backward from the loss gradient in A.dz / A.dzb ([rows x kOutPad]) into s->grad
+void backward(mcs_surrogate* s, Acts& A, int rows, cudaStream_t st) {
+  for (int l = kLayers - 1; l >= 0; l--) {
+    const int K = kK[l], N = kN[l];
+    const bf16* ain = l == 0 ? A.xb : A.a[l - 1];
+    // dW = a_in^T dz ; db = colsum(dz)
+    gemm(st, ain, 1, K, A.dzb, N, 1, s->grad + kLay.W[l], N, K, N, rows, false);
+    col_sum<<<N, 256, 0, st>>>(A.dz, rows, N, s->grad + kLay.b[l]);
+    if (l > 0) {
+      // dh = dz W^T ; dz_prev = dh * silu'(z_prev)
+      gemm(st, A.dzb, N, 1, s->Wb[l], 1, N, A.dh, K, rows, K, N, false);
+      const long n = (long)rows * K;
+      silu_back<<<blocks(n, 256), 256, 0, st>>>(A.dh, A.z[l - 1], n, A.dz, A.dzb);
+    }
+  }
+}
+
+// loss (summed, on the device) and its gradient for rows already gathered
+void loss_grad(mcs_surrogate* s, Acts& A, int rows, cudaStream_t st) {
+  forward(s, A, rows, st);
+  nll_loss<<<blocks(rows, 256), 256, 0, st>>>(A.z[kLayers - 1], A.yb, rows, A.dz, A.dzb,
+                                              s->loss);
+  backward(s, A, rows, st);
+}
+
+}  // namespace
+
+// ---- internal entry points used by the guided solve (mcs_api.cu) ----
+// Allocates the inference buffers once (before any stream capture that uses them).
+int surrogate_reserve(mcs_surrogate* s) { return ensure_acts(s->inf, kInferRows); }
+
+int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d_mu,
+                             float* d_sigma, float2* d_guide, const mcs_guide_opts* g,
+                             cudaStream_t st) {
+  const int chunk = kInferRows;
+  int rc = surrogate_reserve(s);
+  if (rc) return rc;
+  Acts& A = s->inf;
+  for (long off = 0; off < n; off += chunk) {
+    const int rows = (int)std::min<long>(chunk, n - off);
+    gather_rows<<<blocks((long)rows * kInPad, 256), 256, 0, st>>>(
+        dX, nullptr, off, rows, n, s->params + kLay.mean, s->params + kLay.stdv, nullptr, A.xb,
+        nullptr);
+    forward(s, A, rows, st);
+    predict_out<<<blocks(rows, 256), 256, 0, st>>>(
+        A.z[kLayers - 1], rows, d_mu ? d_mu + off : nullptr, d_sigma ? d_sigma + off : nullptr,
+        d_guide ? d_guide + off : nullptr, g ? g->z : 0.f, g ? g->hw_min : 0.f,
+        g ? g->hw_max : 0.f, g ? g->hw_direct : 0.f);
+  }
+  MCS_CUDA_RET(cudaGetLastError());
+  return MCS_OK;
+}
+
+mcs_ctx* surrogate_ctx(mcs_surrogate* s) { return s->ctx; }
+std::mutex& surrogate_mutex(mcs_surrogate* s) { return s->mu; }
+void surrogate_hold(mcs_surrogate* s, int delta) { s->plans += delta; }
+
+}  // namespace mcs
+
+extern "C" {
+
+void mcs_default_train_opts(mcs_train_opts* o) {
+  if (!o) return;
+  o->epochs = 20;
+  o->batch = 4096;
+  o->lr = 1e-3f;
+  o->beta1 = 0.9f;
+  o->beta2 = 0.999f;
+  o->eps = 1e-8f;
+  o->seed = 1;
+  o->warm = 0;
+  o->keep_best = 1;
+}
+
+void mcs_default_guide_opts(mcs_guide_opts* o) {
+  if (!o) return;
+  o->z = 2.0f;
+  o->hw_min = 0.13976194f;  // log(1.15)
+  o->hw_max = 0.40546511f;  // log(1.5)
+  o->hw_direct = 0.69314718f;  // log(2)
+  o->refine = 3;
+  o->pad = 0;
+}
+
+int mcs_surrogate_create(mcs_ctx* ctx, uint64_t seed, mcs_surrogate** out) {
+  if (!ctx || !out) return fail(MCS_ERR_ARG, "NULL ctx or surrogate pointer");
+  *out = nullptr;
+  MCS_CUDA_RET(cudaSetDevice(ctx_device(ctx)));
+  mcs_surrogate* s = new mcs_surrogate();
+  s->ctx = ctx;
+  s->seed = seed;
+  int rc;
+  if ((rc = dalloc(&s->params, kLay.total)) || (rc = dalloc(&s->grad, kLay.total)) ||
+      (rc = dalloc(&s->m, kLay.total)) || (rc = dalloc(&s->v, kLay.total)) ||
+      (rc = dalloc(&s->loss, 1))) {
+    mcs_surrogate_destroy(s);
+    return rc;
+  }
+  for (int l = 0; l < kLayers; l++)
+    if ((rc = dalloc(&s->Wb[l], (size_t)kK[l] * kN[l]))) {
+      mcs_surrogate_destroy(s);
+      return rc;
+    }
+  std::vector<float> p;
+  init_host(p, seed);
+  if ((rc = upload_params(s, p.data())) || (rc = cast_weights(s, ctx_stream(ctx))) ||
+      (rc = cudaStreamSynchronize(ctx_stream(ctx)) == cudaSuccess ? 0
+                                                                  : fail(MCS_ERR_CUDA, "init failed"))) {
+    mcs_surrogate_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return MCS_OK;
+}
+
+int mcs_surrogate_destroy(mcs_surrogate* s) {
+  if (!s) return MCS_OK;
+  if (s->plans.load() > 0)
+    return fail(MCS_ERR_STATE, "%d guided plan(s) still use this surrogate", s->plans.load());
+  cudaSetDevice(ctx_device(s->ctx));
+  cudaStreamSynchronize(ctx_stream(s->ctx));
+  free_acts(s->inf);
+  free_acts(s->tr);
+  cudaFree(s->params);
+  cudaFree(s->grad);
+  cudaFree(s->m);
+  cudaFree(s->v);
+  cudaFree(s->loss);
+  for (int l = 0; l < kLayers; l++) cudaFree(s->Wb[l]);
+  delete s;
+  return MCS_OK;
+}
+
+int mcs_surrogate_get_params(mcs_surrogate* s, float* out, size_t* n) {
+  if (!s || !n) return fail(MCS_ERR_ARG, "NULL surrogate or size");
+  if (!out) {
+    *n = kLay.total;
+    return MCS_OK;
+  }
+  if (*n < kLay.total) return fail(MCS_ERR_ARG, "buffer holds %zu floats, %zu needed", *n, kLay.total);
+  std::lock_guard<std::mutex> lk(s->mu);
+  MCS_CUDA_RET(cudaSetDevice(ctx_device(s->ctx)));
+  MCS_CUDA_RET(cudaStreamSynchronize(ctx_stream(s->ctx)));
+  MCS_CUDA_RET(cudaMemcpy(out, s->params, kLay.total * sizeof(float), cudaMemcpyDeviceToHost));
+  *n = kLay.total;
+  return MCS_OK;
+}
+
+int mcs_surrogate_set_params(mcs_surrogate* s, const float* in, size_t n) {
+  if (!s || !in) return fail(MCS_ERR_ARG, "NULL surrogate or parameters");
+  if (n != kLay.total) return fail(MCS_ERR_ARG, "expected %zu floats, got %zu", kLay.total, n);
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(in[i])) return fail(MCS_ERR_ARG, "parameter %zu is not finite", i);
+  for (int c = 0; c < kIn; c++)
+    if (!(in[kLay.stdv + c] > 0)) return fail(MCS_ERR_ARG, "feature scale %d must be > 0", c);
+  std::lock_guard<std::mutex> lk(s->mu);
+  MCS_CUDA_RET(cudaSetDevice(ctx_device(s->ctx)));
+  cudaStreamSynchronize(ctx_stream(s->ctx));
+  int rc = upload_params(s, in);
+  if (!rc) rc = cast_weights(s, ctx_stream(s->ctx));
+  if (!rc) MCS_CUDA_RET(cudaStreamSynchronize(ctx_stream(s->ctx)));
+  s->trained = true;
+  return rc;
+}
+
+int mcs_surrogate_grad(mcs_surrogate* s, const float* X, const float* y, size_t n, float* loss,
+                       float* grad) {
+  if (!s || !X || !y || !loss || !grad || n == 0 || n > (1u << 20))
+    return fail(MCS_ERR_ARG, "bad arguments to mcs_surrogate_grad");
+  std::lock_guard<std::mutex> lk(s->mu);
+  MCS_CUDA_RET(cudaSetDevice(ctx_device(s->ctx)));
+  int rc = ensure_acts(s->tr, (int)n);
+  if (rc) return rc;
+  float *dX = nullptr, *dy = nullptr;
+  if ((rc = dalloc(&dX, n * kIn)) || (rc = dalloc(&dy, n))) {
+    cudaFree(dX);
+    return rc;
+  }
+  cudaStream_t st = ctx_stream(s->ctx);
+  cudaMemcpyAsync(dX, X, n * kIn * sizeof(float), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dy, y, n * sizeof(float), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(s->loss, 0, sizeof(float), st);
+  cudaMemsetAsync(s->grad, 0, kLay.total * sizeof(float), st);
+  gather_rows<<<blocks((long)n * kInPad, 256), 256, 0, st>>>(
+      dX, nullptr, 0, (int)n, (long)n, s->params + kLay.mean, s->params + kLay.stdv, dy,
+      s->tr.xb, s->tr.yb);
+  loss_grad(s, s->tr, (int)n, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(grad, s->grad, kLay.total * sizeof(float), cudaMemcpyDeviceToHost);
+  float ls = 0.f;
+  if (e == cudaSuccess) e = cudaMemcpy(&ls, s->loss, sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dX);
+  cudaFree(dy);
+  if (e != cudaSuccess) return fail(MCS_ERR_CUDA, "gradient failed: %s", cudaGetErrorString(e));
+  *loss = ls / (float)n;
+  return MCS_OK;
+}
+
+int mcs_surrogate_train(mcs_surrogate* s, const float* X, const float* y, size_t n,
+                        const float* Xv, const float* yv, size_t nv, const mcs_train_opts* o,
+                        float* train_loss, float* val_loss) {
+  if (!s || !X || !y || !o || n == 0) return fail(MCS_ERR_ARG, "bad arguments to train");
+  if (o->batch < 16 || o->batch > 65536 || o->epochs < 1 || !(o->lr > 0))
+    return fail(MCS_ERR_ARG, "train options out of range");
+  if (nv && (!Xv || !yv)) return fail(MCS_ERR_ARG, "validation arrays missing");
+  if (n > (size_t)INT32_MAX || nv > (size_t)INT32_MAX) return fail(MCS_ERR_ARG, "too many rows");
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(y[i])) return fail(MCS_ERR_ARG, "target %zu is not finite", i);
+  std::lock_guard<std::mutex> lk(s->mu);
+  MCS_CUDA_RET(cudaSetDevice(ctx_device(s->ctx)));
+  int rc = MCS_OK;
+  if (!o->warm) {
+    // feature normalisation from the training set, fresh weights and Adam state
+    std::vector<double> mean(kIn, 0.0), var(kIn, 0.0);
+    for (size_t i = 0; i < n; i++)
+      for (int c = 0; c < kIn; c++) mean[c] += X[i * kIn + c];
+    for (int c = 0; c < kIn; c++) mean[c] /= (double)n;
+    for (size_t i = 0; i < n; i++)
+      for (int c = 0; c < kIn; c++) {
+        const double d = X[i * kIn + c] - mean[c];
+        var[c] += d * d;
+      }
+    std::vector<float> p;
+    init_host(p, s->seed);
+    for (int c = 0; c < kIn; c++) {
+      p[kLay.mean + c] = (float)mean[c];
+      p[kLay.stdv + c] = (float)std::max(1e-6, std::sqrt(var[c] / (double)n));
+    }
+    cudaStreamSynchronize(ctx_stream(s->ctx));
+    rc = upload_params(s, p.data());
+    if (!rc) rc = cast_weights(s, ctx_stream(s->ctx));
+  }
+  const int B = o->batch;
+  const bool keep = o->keep_best && nv > 0 && val_loss != nullptr;
+  if (!rc) rc = ensure_acts(s->tr, B);
+  float *dX = nullptr, *dy = nullptr, *dXv = nullptr, *dyv = nullptr, *best = nullptr;
+  int32_t* dperm = nullptr;
+  if (!rc && ((rc = dalloc(&dX, n * kIn)) || (rc = dalloc(&dy, n)) ||
+              (rc = dalloc(&dperm, n)) || (rc = dalloc(&dXv, std::max<size_t>(nv, 1) * kIn)) ||
+              (rc = dalloc(&dyv, std::max<size_t>(nv, 1))) ||
+              (keep && (rc = dalloc(&best, kLay.total))))) {
+  }
+  auto cleanup = [&]() {
+    cudaFree(dX);
+    cudaFree(dy);
+    cudaFree(dperm);
+    cudaFree(dXv);
+    cudaFree(dyv);
+    cudaFree(best);
+  };
+  if (rc) {
+    cleanup();
+    return rc;
+  }
+  cudaStream_t st = ctx_stream(s->ctx);
+  cudaStreamSynchronize(st);
+  cudaMemcpy(dX, X, n * kIn * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(dy, y, n * sizeof(float), cudaMemcpyHostToDevice);
+  if (nv) {
+    cudaMemcpy(dXv, Xv, nv * kIn * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(dyv, yv, nv * sizeof(float), cudaMemcpyHostToDevice);
+  }
+  Acts& A = s->tr;
+  // the shuffle stream continues across warm-started calls
+  Rng rng{s->seed * 0x2545F4914F6CDD1DULL + 7 + (uint64_t)s->step * 0x9E3779B97F4A7C15ULL};
+  float best_loss = INFINITY;
+  std::vector<int32_t> perm(n);
+  const long steps = (long)(n / (size_t)B);
+  const long trainable = (long)(kLay.total - kLay.W[0]);
+  for (int ep = 0; ep < o->epochs && !rc; ep++) {
+    for (size_t i = 0; i < n; i++) perm[i] = (int32_t)i;
+    for (size_t i = n - 1; i > 0; i--) std::swap(perm[i], perm[rng.next() % (i + 1)]);
+    cudaMemcpyAsync(dperm, perm.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(s->loss, 0, sizeof(float), st);
+    for (long k = 0; k < std::max<long>(steps, 1); k++) {
+      const int rows = steps ? B : (int)n;
+      gather_rows<<<blocks((long)rows * kInPad, 256), 256, 0, st>>>(
+          dX, dperm, k * (long)B, rows, (long)n, s->params + kLay.mean, s->params + kLay.stdv, dy,
+          A.xb, A.yb);
+      loss_grad(s, A, rows, st);
+      s->step++;
+      const float c1 = 1.f - std::pow(o->beta1, (float)s->step);
+      const float c2 = 1.f - std::pow(o->beta2, (float)s->step);
+      adam<<<blocks(trainable, 256), 256, 0, st>>>(s->params + kLay.W[0], s->m + kLay.W[0],
+                                                   s->v + kLay.W[0], s->grad + kLay.W[0],
+                                                   trainable, o->lr, o->beta1, o->beta2, o->eps,
+                                                   c1, c2);
+      rc = cast_weights(s, st);
+      if (rc) break;
+    }
+    float ls = 0.f;
+    cudaError_t e = cudaMemcpyAsync(&ls, s->loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // (the host permutation is reused)
+    if (e != cudaSuccess) {
+      rc = fail(MCS_ERR_CUDA, "training failed: %s", cudaGetErrorString(e));
+      break;
+    }
+    if (train_loss) train_loss[ep] = ls / (float)(steps ? steps * B : (long)n);
+    if (val_loss && nv) {
+      cudaMemsetAsync(s->loss, 0, sizeof(float), st);
+      for (size_t off = 0; off < nv; off += (size_t)B) {
+        const int rows = (int)std::min<size_t>((size_t)B, nv - off);
+        gather_rows<<<blocks((long)rows * kInPad, 256), 256, 0, st>>>(
+            dXv, nullptr, (long)off, rows, (long)nv, s->params + kLay.mean,
+            s->params + kLay.stdv, dyv, A.xb, A.yb);
+        forward(s, A, rows, st);
+        nll_loss<<<blocks(rows, 256), 256, 0, st>>>(A.z[kLayers - 1], A.yb, rows, A.dz, A.dzb,
+                                                    s->loss);
+      }
+      e = cudaMemcpyAsync(&ls, s->loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        rc = fail(MCS_ERR_CUDA, "validation failed: %s", cudaGetErrorString(e));
+        break;
+      }
+      val_loss[ep] = ls / (float)nv;
+      if (keep && val_loss[ep] < best_loss) {
+        best_loss = val_loss[ep];
+        cudaMemcpyAsync(best, s->params, kLay.total * sizeof(float), cudaMemcpyDeviceToDevice,
+                        st);
+      }
+    }
+  }
+  if (!rc && keep && best_loss < INFINITY) {
+    cudaMemcpyAsync(s->params, best, kLay.total * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    rc = cast_weights(s, st);
+  }
+  cudaStreamSynchronize(st);
+  cleanup();
+  if (!rc) s->trained = true;
+  return rc;
+}
+
+int mcs_surrogate_predict(mcs_surrogate* s, const float* X, size_t n, float* mu, float* sigma) {
+  if (!s || (n && (!X || !mu || !sigma))) return fail(MCS_ERR_ARG, "bad arguments to predict");
+  if (n == 0) return MCS_OK;
+  std::lock_guard<std::mutex> lk(s->mu);
+  MCS_CUDA_RET(cudaSetDevice(ctx_device(s->ctx)));
+  float *dX = nullptr, *dmu = nullptr, *dsg = nullptr;
+  int rc;
+  if ((rc = dalloc(&dX, n * kIn)) || (rc = dalloc(&dmu, n)) || (rc = dalloc(&dsg, n))) {
+    cudaFree(dX);
+    cudaFree(dmu);
+    return rc;
+  }
+  cudaStream_t st = ctx_stream(s->ctx);
+  cudaMemcpyAsync(dX, X, n * kIn * sizeof(float), cudaMemcpyHostToDevice, st);
+  rc = surrogate_predict_device(s, dX, (long)n, dmu, dsg, nullptr, nullptr, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (!rc && e == cudaSuccess) e = cudaMemcpy(mu, dmu, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (!rc && e == cudaSuccess)
+    e = cudaMemcpy(sigma, dsg, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dX);
+  cudaFree(dmu);
+  cudaFree(dsg);
+  if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "predict failed: %s", cudaGetErrorString(e));
+  return rc;
+}
+
+}  // extern "C"

@@ -7,18 +7,23 @@ The functions mirror the reference's JavaScript API for this path:
   StabWorker (the message protocol)   src/stabworker.js:1-15
   lobeLimit (stabilityLobes + alimAt) src/sld.js:23-76
 
+Surrogate (an MLP trained on the solver's own limits) guides the bisection of
+Context.solve_guided and guided plans; mcs.surrogate trains and stores one.
+
 All compute runs in the CUDA library; a missing library or device raises.
 """
 from ._abi import (CHATTER_IDX, DEFAULTS, make_material, make_modal, make_opts, make_setup,
                    make_tool)
-from ._lib import Context, Job, MCSError, Plan, default_context, load
+from ._lib import (Context, Job, MCSError, Plan, Surrogate, default_context,
+                   default_guide_opts, default_train_opts, load)
 from .sld import lobeLimit, lobeLimits
 from .stabtd import chatterAt, chatterIndex, timeDomainLimit, timeDomainLimits
 from .worker import StabWorker
 
 __all__ = [
-    "CHATTER_IDX", "DEFAULTS", "Context", "Job", "MCSError", "Plan", "StabWorker",
-    "chatterAt", "chatterIndex", "default_context", "load", "lobeLimit", "lobeLimits",
+    "CHATTER_IDX", "DEFAULTS", "Context", "Job", "MCSError", "Plan", "StabWorker", "Surrogate",
+    "chatterAt", "chatterIndex", "default_context", "default_guide_opts",
+    "default_train_opts", "load", "lobeLimit", "lobeLimits",
     "make_material", "make_modal", "make_opts", "make_setup", "make_tool", "timeDomainLimit",
     "timeDomainLimits",
 ]

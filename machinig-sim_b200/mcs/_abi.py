@@ -276,3 +276,30 @@ def as_records(items, dtype) -> np.ndarray:
 
 def opts_record(o: Opts) -> np.ndarray:
     return np.frombuffer(bytes(o), dtype=OPTS_DTYPE).copy()
+
+
+# ---------------------------------------------------------------- surrogate
+FEATURES = 20
+PATH_GUIDED, PATH_FALLBACK, PATH_DIRECT, PATH_OPEN = 0, 1, 2, 3
+PATH_NAMES = {PATH_GUIDED: "guided", PATH_FALLBACK: "fallback", PATH_DIRECT: "direct",
+              PATH_OPEN: "open"}
+
+
+class TrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("seed", C.c_uint64), ("warm", C.c_int32), ("keep_best", C.c_int32)]
+
+
+class GuideOpts(C.Structure):
+    _fields_ = [("z", C.c_float), ("hw_min", C.c_float), ("hw_max", C.c_float),
+                ("hw_direct", C.c_float), ("refine", C.c_int32), ("pad", C.c_int32)]
+
+
+class GuideInfo(C.Structure):
+    _fields_ = [("mu", C.c_float), ("sigma", C.c_float), ("path", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+GUIDE_INFO_DTYPE = np.dtype([("mu", "<f4"), ("sigma", "<f4"), ("path", "<i4"), ("pad", "<i4")])
+assert GUIDE_INFO_DTYPE.itemsize == C.sizeof(GuideInfo)

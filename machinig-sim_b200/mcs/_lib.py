@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import threading
+import weakref
 from pathlib import Path
 from typing import Sequence
 
@@ -23,7 +24,13 @@ EXPORTS = (
     "mcs_solve", "mcs_chatter_at", "mcs_plan_create", "mcs_plan_execute", "mcs_plan_results",
     "mcs_plan_info_get", "mcs_plan_destroy", "mcs_solve_async", "mcs_job_poll",
     "mcs_job_cancel", "mcs_job_wait", "mcs_job_free", "mcs_lobes_alim", "mcs_solve_noalloc",
+    "mcs_default_train_opts", "mcs_default_guide_opts", "mcs_features", "mcs_surrogate_create",
+    "mcs_surrogate_destroy", "mcs_surrogate_train", "mcs_surrogate_predict", "mcs_surrogate_grad",
+    "mcs_surrogate_get_params", "mcs_surrogate_set_params", "mcs_solve_guided",
+    "mcs_plan_create_guided", "mcs_plan_guide_info",
 )
+_VOID = ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free",
+         "mcs_default_train_opts", "mcs_default_guide_opts")
 
 _LIB = None
 _LOCK = threading.Lock()
@@ -73,8 +80,24 @@ def load(path: Path | str | None = None):
         L.mcs_job_free.restype = None
         L.mcs_lobes_alim.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, vp]
         L.mcs_solve_noalloc.argtypes = batch + [vp]
+        L.mcs_default_train_opts.argtypes = [P(A.TrainOpts)]
+        L.mcs_default_train_opts.restype = None
+        L.mcs_default_guide_opts.argtypes = [P(A.GuideOpts)]
+        L.mcs_default_guide_opts.restype = None
+        L.mcs_features.argtypes = batch[1:] + [vp]
+        L.mcs_surrogate_create.argtypes = [vp, C.c_uint64, P(vp)]
+        L.mcs_surrogate_destroy.argtypes = [vp]
+        L.mcs_surrogate_train.argtypes = [vp, vp, vp, C.c_size_t, vp, vp, C.c_size_t,
+                                          P(A.TrainOpts), vp, vp]
+        L.mcs_surrogate_predict.argtypes = [vp, vp, C.c_size_t, vp, vp]
+        L.mcs_surrogate_grad.argtypes = [vp, vp, vp, C.c_size_t, vp, vp]
+        L.mcs_surrogate_get_params.argtypes = [vp, vp, P(C.c_size_t)]
+        L.mcs_surrogate_set_params.argtypes = [vp, vp, C.c_size_t]
+        L.mcs_solve_guided.argtypes = [vp, vp] + batch[1:] + [P(A.GuideOpts), vp, vp]
+        L.mcs_plan_create_guided.argtypes = [vp, vp] + batch[1:] + [P(A.GuideOpts), P(vp)]
+        L.mcs_plan_guide_info.argtypes = [vp, vp]
         for name in EXPORTS:
-            if name not in ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free"):
+            if name not in _VOID:
                 getattr(L, name).restype = C.c_int
         if path is None:
             _LIB = L
@@ -114,15 +137,29 @@ class Batch:
 
 
 class Plan:
-    """Device-resident solve batch launched as a captured CUDA graph."""
+    """Device-resident solve batch launched as a captured CUDA graph (optionally guided by
+    a surrogate, which must outlive the plan)."""
 
-    def __init__(self, ctx: "Context", batch: Batch, opts: A.Opts):
+    def __init__(self, ctx: "Context", batch: Batch, opts: A.Opts, surrogate=None,
+                 guide: A.GuideOpts | None = None):
         self.ctx = ctx
         self.batch = batch
         self.n = len(batch.points)
+        self.surrogate = surrogate
         h = C.c_void_p()
-        check(ctx._L.mcs_plan_create(ctx._h, *batch.args(), C.byref(opts), C.byref(h)))
+        if surrogate is None:
+            check(ctx._L.mcs_plan_create(ctx._h, *batch.args(), C.byref(opts), C.byref(h)))
+        else:
+            g = guide if guide is not None else default_guide_opts()
+            check(ctx._L.mcs_plan_create_guided(ctx._h, surrogate._h, *batch.args(),
+                                                C.byref(opts), C.byref(g), C.byref(h)))
         self._h = h
+        ctx._adopt(self)
+
+    def guide_info(self) -> np.ndarray:
+        out = np.zeros(max(1, self.n), dtype=A.GUIDE_INFO_DTYPE)
+        check(self.ctx._L.mcs_plan_guide_info(self._h, _ptr(out)))
+        return out[: self.n]
 
     def execute(self) -> None:
         check(self.ctx._L.mcs_plan_execute(self._h))
@@ -161,6 +198,7 @@ class Job:
         check(ctx._L.mcs_solve_async(ctx._h, *batch.args(), C.byref(opts), _ptr(self.out),
                                      C.byref(h)))
         self._h = h
+        ctx._adopt(self)
 
     def poll(self) -> tuple[int, bool]:
         done = C.c_size_t()
@@ -200,6 +238,11 @@ class Context:
         check(self._L.mcs_create(C.byref(h), int(device)))
         self._h = h
         self.device = device
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, obj) -> None:
+        """Plans, jobs and surrogates of this context are closed before it."""
+        self._children.add(obj)
 
     @property
     def stream(self) -> int:
@@ -219,8 +262,27 @@ class Context:
                                      _ptr(out)))
         return out[: len(t)]
 
-    def plan(self, setups, modals, points, opts: A.Opts) -> Plan:
-        return Plan(self, Batch(setups, modals, points), opts)
+    def plan(self, setups, modals, points, opts: A.Opts, surrogate=None,
+             guide: A.GuideOpts | None = None) -> Plan:
+        return Plan(self, Batch(setups, modals, points), opts, surrogate, guide)
+
+    def features(self, setups, modals, points, opts: A.Opts) -> np.ndarray:
+        b = Batch(setups, modals, points)
+        out = np.zeros((max(1, len(b.points)), A.FEATURES), dtype=np.float32)
+        check(self._L.mcs_features(*b.args(), C.byref(opts), _ptr(out)))
+        return out[: len(b.points)]
+
+    def solve_guided(self, surrogate, setups, modals, points, opts: A.Opts,
+                     guide: A.GuideOpts | None = None):
+        """(results, guide info) of the surrogate-guided solve."""
+        b = Batch(setups, modals, points)
+        n = len(b.points)
+        out = np.zeros(max(1, n), dtype=A.RESULT_DTYPE)
+        info = np.zeros(max(1, n), dtype=A.GUIDE_INFO_DTYPE)
+        g = guide if guide is not None else default_guide_opts()
+        check(self._L.mcs_solve_guided(self._h, surrogate._h, *b.args(), C.byref(opts),
+                                       C.byref(g), _ptr(out), _ptr(info)))
+        return out[:n], info[:n]
 
     def solve_async(self, setups, modals, points, opts: A.Opts) -> Job:
         return Job(self, Batch(setups, modals, points), opts)
@@ -236,7 +298,90 @@ class Context:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
+            kids = list(getattr(self, "_children", ()))
+            # plans and jobs first: a guided plan holds its surrogate
+            for k in sorted(kids, key=lambda o: isinstance(o, Surrogate)):
+                k.close()
             self._L.mcs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def default_train_opts() -> A.TrainOpts:
+    o = A.TrainOpts()
+    load().mcs_default_train_opts(C.byref(o))
+    return o
+
+
+def default_guide_opts() -> A.GuideOpts:
+    o = A.GuideOpts()
+    load().mcs_default_guide_opts(C.byref(o))
+    return o
+
+
+class Surrogate:
+    """The MLP surrogate on a context's device (mcs_surrogate_*)."""
+
+    def __init__(self, ctx: Context, seed: int = 1):
+        self.ctx = ctx
+        self._L = ctx._L
+        h = C.c_void_p()
+        check(self._L.mcs_surrogate_create(ctx._h, int(seed), C.byref(h)))
+        self._h = h
+        ctx._adopt(self)
+
+    def train(self, X, y, Xv=None, yv=None, opts: A.TrainOpts | None = None):
+        """Returns (train_loss[epochs], val_loss[epochs])."""
+        o = opts if opts is not None else default_train_opts()
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        nv = 0 if Xv is None else len(Xv)
+        Xv = np.ascontiguousarray(Xv if nv else np.zeros((1, A.FEATURES)), dtype=np.float32)
+        yv = np.ascontiguousarray(yv if nv else np.zeros(1), dtype=np.float32)
+        tl = np.zeros(o.epochs, dtype=np.float32)
+        vl = np.zeros(o.epochs, dtype=np.float32)
+        check(self._L.mcs_surrogate_train(self._h, _ptr(X), _ptr(y), len(X), _ptr(Xv), _ptr(yv),
+                                          nv, C.byref(o), _ptr(tl), _ptr(vl)))
+        return tl, vl
+
+    def predict(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        mu = np.zeros(max(1, len(X)), dtype=np.float32)
+        sg = np.zeros(max(1, len(X)), dtype=np.float32)
+        check(self._L.mcs_surrogate_predict(self._h, _ptr(X), len(X), _ptr(mu), _ptr(sg)))
+        return mu[: len(X)], sg[: len(X)]
+
+    def grad(self, X, y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        n = C.c_size_t()
+        check(self._L.mcs_surrogate_get_params(self._h, None, C.byref(n)))
+        g = np.zeros(n.value, dtype=np.float32)
+        loss = C.c_float()
+        check(self._L.mcs_surrogate_grad(self._h, _ptr(X), _ptr(y), len(X), C.byref(loss),
+                                         _ptr(g)))
+        return float(loss.value), g
+
+    def get_params(self) -> np.ndarray:
+        n = C.c_size_t()
+        check(self._L.mcs_surrogate_get_params(self._h, None, C.byref(n)))
+        out = np.zeros(n.value, dtype=np.float32)
+        check(self._L.mcs_surrogate_get_params(self._h, _ptr(out), C.byref(n)))
+        return out
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(self._L.mcs_surrogate_set_params(self._h, _ptr(p), len(p)))
+
+    def close(self) -> None:
+        """Raises MCSError (MCS_ERR_STATE) while a guided plan still uses the surrogate."""
+        if getattr(self, "_h", None):
+            check(self._L.mcs_surrogate_destroy(self._h))
             self._h = None
 
     def __del__(self):
