@@ -148,6 +148,91 @@ def cpu_baseline(wl, target_s: float = 15.0) -> dict:
                       f"stabtd.js/cutting.js, {cores} threads on {cpu_model()}"}
 
 
+def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool) -> dict:
+    """Surrogate-guided serving: 65536 seeded hetero queries (30 % of the setups outside the
+    training seeds), the trained model's guided plan against the plain plan on the same
+    queries, with agreement against the plain GPU bisection and, on a seeded 512-query
+    subset, against the FP64 restatement of the reference on the host."""
+    from mcs import _abi as A
+    from mcs import surrogate as SG
+    from mcs import workloads as W
+
+    if not SG.DEFAULT_MODEL.exists():
+        return {"unavailable": f"no trained model at {SG.DEFAULT_MODEL.name}"}
+    sv = W.serve()
+    sur = SG.load(ctx)
+    rec = SG.record_of()
+
+    def run(plan):
+        plan.execute()  # warm-up (graph upload)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            flush.fill_(7)
+        a.record(stream)
+        plan.execute()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), plan.results()
+
+    with ClockSampler(device) as clk:
+        pp = ctx.plan(sv.setups, sv.modals, sv.points, sv.opts)
+        plain_ms, plain = run(pp)
+        pp.close()
+        gp = ctx.plan(sv.setups, sv.modals, sv.points, sv.opts, surrogate=sur)
+        guided_ms, gres = run(gp)
+        info = gp.guide_info()
+        gp.close()
+    sur.close()
+    path = info["path"]
+    both_open = (gres["open"] == 1) & (plain["open"] == 1)
+    rel = np.where(both_open, 0.0, np.abs(gres["alim"] / plain["alim"] - 1))
+    out = np.asarray(sv.meta["outside"])
+    sub = np.asarray(sv.meta["fp64_subset"])
+    # FP64 references on the subset: the GPU FP64 bisection and the host FP64 restatement
+    o64 = A.make_opts(precision="fp64")
+    for f in ("a_min", "a_max", "iters", "revs", "nonlinear", "honor_runout", "steps_per_tooth",
+              "slices", "chatter_idx"):
+        setattr(o64, f, getattr(sv.opts, f))
+    g64 = ctx.solve(sv.setups, sv.modals, sv.points[sub], o64)
+
+    def within(a, b):
+        op = (a["open"] == 1) & (b["open"] == 1)
+        return float(np.mean(op | (np.abs(a["alim"] / b["alim"] - 1) <= 0.02)))
+
+    res = {
+        "workload": f"serve: {sv.n} seeded hetero (setup, speed) queries, "
+                    f"{float(out.mean()):.0%} outside the training seeds",
+        "value": sv.n / (guided_ms / 1e3), "unit": UNIT,
+        "plain_value": sv.n / (plain_ms / 1e3), "speedup_vs_plain": plain_ms / guided_ms,
+        "trials_ratio": float(gres["trials"].sum() / plain["trials"].sum()),
+        "paths": {A.PATH_NAMES[k]: float(np.mean(path == k)) for k in range(4)},
+        "fallback_rate": float(np.mean(path == A.PATH_FALLBACK)),
+        "within_2pct_of_plain": float(np.mean(rel <= 0.02)),
+        "within_2pct_of_plain_outside_seeds": float(np.mean(rel[out] <= 0.02)),
+        "median_rel_err_vs_plain_guided": float(np.median(rel[path == A.PATH_GUIDED]))
+        if np.any(path == A.PATH_GUIDED) else None,
+        "fp64_subset": len(sub),
+        "within_2pct_of_gpu_fp64": within(gres[sub], g64),
+        "plain_within_2pct_of_gpu_fp64": within(plain[sub], g64),
+        "model": {"file": SG.DEFAULT_MODEL.name, "epochs": rec.get("epochs"),
+                  "train_points": rec.get("train_points"),
+                  "val_within_15pct": rec.get("val_within_15pct")},
+        "clocks": clk.summary(),
+    }
+    if not no_cpu:
+        import pyoracle as O
+
+        setups = [A.Setup.from_buffer_copy(r.tobytes()) for r in sv.setups]
+        modals = [A.Modal.from_buffer_copy(r.tobytes()) for r in sv.modals]
+        pts = sv.points[sub]
+        P = (A.Point * len(pts)).from_buffer_copy(pts.tobytes())
+        r64, _ = O.solve_batch(setups, modals, P, sv.opts, nthreads=cpu_cores())
+        res["within_2pct_of_cpu_fp64"] = within(gres[sub], r64)
+        res["plain_within_2pct_of_cpu_fp64"] = within(plain[sub], r64)
+    return res
+
+
 def reference_arm(args) -> int:
     rank, world, _ = env_rank()
     if rank != 0:
@@ -312,6 +397,8 @@ def ours(args) -> int:
     line = None
     if rank == 0:
         cpu = cpu_baseline(wl) if world == 1 and not args.no_cpu else None
+        guided = (guided_serve(ctx, torch, stream, flush, device, args.no_cpu)
+                  if world == 1 and not args.no_guided else None)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -336,6 +423,7 @@ def ours(args) -> int:
                                  f"out-of-cut reference evaluation; {evals:.3e} evaluations, "
                                  f"{engaged:.3e} in cut per step"},
             "cpu_baseline": cpu,
+            "guided": guided,
             "e2e": e2e,
             "gpu_launches": int(info["kernels"]) * args.steps,
             "clocks": clocks,
@@ -365,6 +453,8 @@ def main(argv=None) -> int:
     ap.add_argument("--points", type=int, default=0,
                     help="solve an evenly spaced subset of the sweep (profiling case)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-guided", action="store_true",
+                    help="skip the surrogate-guided serving leg")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         a.warmup = 3

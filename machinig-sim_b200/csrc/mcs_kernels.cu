@@ -401,83 +401,113 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         if (t.status != MCS_OK) r.status = t.status;
         return t.index > o.chatter_idx;
       };
-      bool done = false;
-      bool top_chatters = false;  // the first plain trial, chatter(a_max), already ran
-      int path = MCS_PATH_DIRECT;
-      if (g.guide != nullptr && g.guide[pi].y >= 0.f) {
-        // surrogate-guided: the plain first trial at a_max (stabtd.js:25) runs as it does
-        // without a guide, so open points come out exactly as in the plain method; then
-        // the bracket exp(mu -+ hw), kept inside [a_min, a_max], must be stable at its
-        // lower and chatter at its upper end and is refined by the same geometric
-        // bisection.  A failed verification falls back to the full bisection.
-        const float2 gd = g.guide[pi];
-        if (!chatter(o.a_max)) {
-          r.alim = o.a_max;
-          r.lo = o.a_max;
-          r.hi = INFINITY;
-          r.open = 1;
-          path = MCS_PATH_OPEN;
-          done = true;
-        } else {
-          top_chatters = true;
-          const double hw = (double)gd.y;
-          double lo = exp((double)gd.x - hw), hi = exp((double)gd.x + hw);
-          if (lo < o.a_min) {  // shift up to start at a_min
-            lo = o.a_min;
-            hi = fmin(fmax(hi, o.a_min * exp(2.0 * hw)), o.a_max);
-          }
-          if (hi > o.a_max) {  // shift down to end at a_max
-            hi = o.a_max;
-            lo = fmax(fmin(lo, o.a_max * exp(-2.0 * hw)), o.a_min);
-          }
-          bool ok = lo < hi;
-          if (ok && hi < o.a_max) ok = chatter(hi);   // a_max is known to chatter
-          if (ok && lo > o.a_min) ok = !chatter(lo);  // a_min is taken as stable, as plain does
-          if (ok) {
-            // enough halvings that the final bracket is no wider than a hw_min bracket's
-            // after `refine` halvings
-            int iters = g.refine;
-            for (double w = log(hi / lo) * 0.5; w > 1.0000001 * (double)g.hw_min; w *= 0.5)
-              iters++;
-            for (int it = 0; it < iters; it++) {
-              const double m = sqrt(lo * hi);
-              if (chatter(m))
-                hi = m;
-              else
-                lo = m;
-            }
+      // timeDomainLimit (stabtd.js:24-32) as a state machine around ONE trial call site
+      // (the trial is inlined once): the plain first trial at a_max, then either the
+      // plain geometric bisection over [a_min, a_max] or, with a surrogate guide, the
+      // bracket exp(mu -+ hw) kept inside [a_min, a_max], verified at its upper (chatter)
+      // and lower (stable) end and refined by the same bisection.  A failed verification
+      // falls back to the plain bisection, whose a_max trial has already run.
+      enum : int { kTop, kGuideHi, kGuideLo, kBisect, kDone };
+      const bool guided = g.guide != nullptr && g.guide[pi].y >= 0.f;
+      int path = guided ? MCS_PATH_GUIDED : MCS_PATH_DIRECT;
+      int state = kTop, it = 0, iters = o.iters;
+      double lo = o.a_min, hi = o.a_max, glo = 0.0, ghi = 0.0;
+      // enter the bisection of [l, h] for n iterations
+      auto bisect = [&](double l, double h, int n) {
+        lo = l;
+        hi = h;
+        it = 0;
+        iters = n;
+        state = kBisect;
+      };
+      auto fallback = [&]() {
+        path = MCS_PATH_FALLBACK;
+        bisect(o.a_min, o.a_max, o.iters);
+      };
+      // enough halvings that the final bracket is no wider than a hw_min bracket's after
+      // `refine` halvings
+      auto refine = [&]() {
+        int n = g.refine;
+        for (double w = log(ghi / glo) * 0.5; w > 1.0000001 * (double)g.hw_min; w *= 0.5) n++;
+        bisect(glo, ghi, n);
+      };
+      while (state != kDone) {
+        if (state == kBisect) {
+          if (it >= iters) {
             r.alim = sqrt(lo * hi);
             r.lo = lo;
             r.hi = hi;
-            path = MCS_PATH_GUIDED;
-            done = true;
-          } else {
-            path = MCS_PATH_FALLBACK;
+            state = kDone;
+            break;
+          }
+          if (path != MCS_PATH_GUIDED && read_cancel(cancel, lane)) {
+            r.status = MCS_ERR_CANCELLED;
+            r.alim = sqrt(lo * hi);
+            r.lo = lo;
+            r.hi = hi;
+            break;
           }
         }
-      }
-      if (!done) {  // the reference's algorithm (stabtd.js:24-32)
-        if (!top_chatters && !chatter(o.a_max)) {
-          r.alim = o.a_max;
-          r.lo = o.a_max;
-          r.hi = INFINITY;
-          r.open = 1;
-        } else {
-          double lo = o.a_min, hi = o.a_max;
-          for (int it = 0; it < o.iters; it++) {
-            if (read_cancel(cancel, lane)) {
-              r.status = MCS_ERR_CANCELLED;
-              break;
+        const double ap = state == kTop       ? o.a_max
+                          : state == kGuideHi ? ghi
+                          : state == kGuideLo ? glo
+                                              : sqrt(lo * hi);
+        const bool c = chatter(ap);
+        switch (state) {
+          case kTop:
+            if (!c) {
+              r.alim = o.a_max;
+              r.lo = o.a_max;
+              r.hi = INFINITY;
+              r.open = 1;
+              if (guided) path = MCS_PATH_OPEN;
+              state = kDone;
+            } else if (!guided) {
+              bisect(o.a_min, o.a_max, o.iters);
+            } else {
+              const float2 gd = g.guide[pi];
+              const double hw = (double)gd.y;
+              glo = exp((double)gd.x - hw);
+              ghi = exp((double)gd.x + hw);
+              if (glo < o.a_min) {  // shift up to start at a_min
+                glo = o.a_min;
+                ghi = fmin(fmax(ghi, o.a_min * exp(2.0 * hw)), o.a_max);
+              }
+              if (ghi > o.a_max) {  // shift down to end at a_max
+                ghi = o.a_max;
+                glo = fmax(fmin(glo, o.a_max * exp(-2.0 * hw)), o.a_min);
+              }
+              if (!(glo < ghi))
+                fallback();
+              else if (ghi < o.a_max)  // a_max is known to chatter
+                state = kGuideHi;
+              else if (glo > o.a_min)  // a_min is taken as stable, as the plain method does
+                state = kGuideLo;
+              else
+                refine();
             }
-            const double m = sqrt(lo * hi);
-            if (chatter(m))
-              hi = m;
+            break;
+          case kGuideHi:
+            if (!c)
+              fallback();
+            else if (glo > o.a_min)
+              state = kGuideLo;
             else
-              lo = m;
-          }
-          r.alim = sqrt(lo * hi);
-          r.lo = lo;
-          r.hi = hi;
+              refine();
+            break;
+          case kGuideLo:
+            if (c)
+              fallback();
+            else
+              refine();
+            break;
+          default:  // kBisect
+            if (c)
+              hi = ap;
+            else
+              lo = ap;
+            it++;
+            break;
         }
       }
       if (g.info != nullptr && lane == 0) {

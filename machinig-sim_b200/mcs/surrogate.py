@@ -39,8 +39,12 @@ def labels(ctx: Context, wl: W.Workload, precision: str = "fp32", chunk: int = 6
 
 
 def train(ctx: Context, wl: W.Workload | None = None, seed: int = 1, epochs: int = 20,
-          batch: int = 4096, log=print):
-    """Labels + training on the seed-split of `wl` (default: the train workload)."""
+          batch: int = 4096, keep_best: bool = False, log=print):
+    """Labels + training on the seed-split of `wl` (default: the train workload).
+
+    keep_best=False keeps the last epoch: serving queries mostly come from training setups
+    at new speeds, where the longer fit predicts better than the epoch of lowest loss on
+    unseen setups."""
     wl = wl if wl is not None else W.train()
     t0 = time.time()
     X = ctx.features(wl.setups, wl.modals, wl.points, wl.opts)
@@ -50,7 +54,7 @@ def train(ctx: Context, wl: W.Workload | None = None, seed: int = 1, epochs: int
     val = val_setup[wl.points["setup"]] if val_setup is not None else np.zeros(wl.n, bool)
     s = Surrogate(ctx, seed)
     o = default_train_opts()
-    o.epochs, o.batch, o.seed = epochs, batch, seed
+    o.epochs, o.batch, o.seed, o.keep_best = epochs, batch, seed, int(keep_best)
     t1 = time.time()
     tl, vl = s.train(X[~val], y[~val], X[val], y[val], o)
     t_train = time.time() - t1
@@ -59,6 +63,7 @@ def train(ctx: Context, wl: W.Workload | None = None, seed: int = 1, epochs: int
     record = {
         "workload": wl.name, "points": int(wl.n), "train_points": int((~val).sum()),
         "val_points": int(val.sum()), "epochs": epochs, "batch": batch, "seed": seed,
+        "keep_best": bool(keep_best),
         "label_seconds": round(t_label, 2), "train_seconds": round(t_train, 2),
         "label_points_per_s": round(wl.n / t_label, 1),
         "train_loss": [float(v) for v in tl], "val_loss": [float(v) for v in vl],
@@ -102,10 +107,12 @@ def main(argv=None) -> int:
     t.add_argument("--batch", type=int, default=4096)
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--device", type=int, default=0)
+    t.add_argument("--keep-best", action="store_true")
     a = ap.parse_args(argv)
     ctx = Context(a.device)
     wl = W.train(n_setups=a.setups, speeds_per_setup=a.speeds)
-    s, rec = train(ctx, wl, seed=a.seed, epochs=a.epochs, batch=a.batch)
+    s, rec = train(ctx, wl, seed=a.seed, epochs=a.epochs, batch=a.batch,
+                   keep_best=a.keep_best)
     save(s, Path(a.out), rec)
     return 0
 

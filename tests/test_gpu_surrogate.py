@@ -224,3 +224,57 @@ def test_surrogate_outlives_its_plans(ctx, trained_small):
     assert len(plan.results()) == 8
     plan.close()
     t.close()
+
+
+def test_keep_best_and_warm_start(ctx, feats):
+    from mcs import Surrogate
+    from mcs._lib import default_train_opts
+
+    _, X = feats
+    Z = (X - X.mean(0)) / (X.std(0) + 1e-6)
+    y = (0.5 * Z[:, 0] - 0.5 * Z[:, 11] + 0.4 * np.sin(2 * Z[:, 4])).astype(np.float32)
+    s = Surrogate(ctx, 9)
+    o = default_train_opts()
+    o.epochs, o.batch, o.lr, o.keep_best = 12, 256, 3e-3, 1
+    tl, vl = s.train(X[:1536], y[:1536], X[1536:], y[1536:], o)
+    # the parameters left are those of the epoch of lowest validation loss
+    loss, _ = s.grad(X[1536:], y[1536:])
+    assert loss == pytest.approx(float(vl.min()), rel=1e-3, abs=1e-4)
+    # a warm start continues from them instead of a fresh initialisation
+    o.warm, o.epochs, o.keep_best = 1, 3, 0
+    tl2, _ = s.train(X[:1536], y[:1536], None, None, o)
+    assert tl2[0] < tl[0]
+    s.close()
+
+
+def test_ablation_trained_model_saves_trials(ctx):
+    """What the trained network gains over the method without it.  On 2048 serving
+    queries the committed model's guided solve needs fewer time-domain trials than the
+    plain bisection, and than the same guided method with an untrained network, while its
+    limits stay within 2 % of the plain ones on at least 99 % of the queries."""
+    from mcs import Surrogate
+    from mcs import surrogate as SG
+    from mcs import workloads as W
+
+    assert SG.DEFAULT_MODEL.exists(), "the trained model is part of the package"
+    sv = W.serve().subset(np.arange(2048))
+    plain = ctx.solve(sv.setups, sv.modals, sv.points, sv.opts)
+    trained = SG.load(ctx)
+    untrained = Surrogate(ctx, 1)
+
+    def within(r):
+        op = (r["open"] == 1) & (plain["open"] == 1)
+        return float(np.mean(op | (np.abs(r["alim"] / plain["alim"] - 1) <= 0.02)))
+
+    rt, it = ctx.solve_guided(trained, sv.setups, sv.modals, sv.points, sv.opts)
+    ru, iu = ctx.solve_guided(untrained, sv.setups, sv.modals, sv.points, sv.opts)
+    tp, tt, tu = plain["trials"].sum(), rt["trials"].sum(), ru["trials"].sum()
+    print(f"trials: plain {tp}, trained {tt} ({tt / tp:.3f}), untrained {tu} ({tu / tp:.3f}); "
+          f"guided fraction trained {np.mean(it['path'] == 0):.3f} untrained "
+          f"{np.mean(iu['path'] == 0):.3f}; within 2 %: trained {within(rt):.4f} untrained "
+          f"{within(ru):.4f}")
+    assert tt < tp
+    assert tt < tu
+    assert within(rt) >= 0.99
+    trained.close()
+    untrained.close()
