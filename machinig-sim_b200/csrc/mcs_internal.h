@@ -106,10 +106,11 @@ struct KernelShape {
 int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                  const PointParams* pts, const int32_t* order, int n, DevOpts opts,
                  mcs_result* out, unsigned int* queue, const volatile int* cancel,
-                 unsigned int* progress, const GuideArgs& guide = GuideArgs());
+                 unsigned int* progress, const GuideArgs& guide = GuideArgs(),
+                 int priority = 0);
 int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                   const PointParams* pts, const TrialItem* items, int n, double chatter_idx,
-                  mcs_trial_result* out, unsigned int* queue);
+                  mcs_trial_result* out, unsigned int* queue, int priority = 0);
 int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm);
 int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm);
 int set_smem_limits();
@@ -118,6 +119,8 @@ int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d
                              float* d_sigma, float2* d_guide, const mcs_guide_opts* g,
                              cudaStream_t st);
 int surrogate_reserve(mcs_surrogate* s);
+// after a synchronise: MCS_ERR_CUDA if an inference kernel timed out waiting for its MMAs
+int surrogate_check(mcs_surrogate* s);
 mcs_ctx* surrogate_ctx(mcs_surrogate* s);
 std::mutex& surrogate_mutex(mcs_surrogate* s);
 // guided plans that hold the surrogate (it cannot be destroyed while any do)

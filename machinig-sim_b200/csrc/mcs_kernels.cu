@@ -618,24 +618,41 @@ int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm) {
   return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, kWarp, smem);
 }
 
+// One-warp blocks with a scheduling priority (lower value = scheduled first), so that the
+// buckets of long points get their SMs before the buckets of short ones fill the device.
+int launch_with_priority(void* f, int grid, int smem, cudaStream_t stream, void** args,
+                         int priority) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kWarp);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributePriority;
+  attr[0].val.priority = priority;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return (int)cudaLaunchKernelExC(&cfg, f, args);
+}
+
 int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                  const PointParams* pts, const int32_t* order, int n, DevOpts opts,
                  mcs_result* out, unsigned int* queue, const volatile int* cancel,
-                 unsigned int* progress, const GuideArgs& guide) {
+                 unsigned int* progress, const GuideArgs& guide, int priority) {
   void* f = pick(true, shape);
   if (!f) return (int)cudaErrorInvalidValue;
   GuideArgs g = guide;
   void* args[] = {&pts, &order, &n, &opts, &out, &queue, &cancel, &progress, &g};
-  return (int)cudaLaunchKernel(f, dim3(grid), dim3(kWarp), args, (size_t)smem, stream);
+  return launch_with_priority(f, grid, smem, stream, args, priority);
 }
 
 int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                   const PointParams* pts, const TrialItem* items, int n, double chatter_idx,
-                  mcs_trial_result* out, unsigned int* queue) {
+                  mcs_trial_result* out, unsigned int* queue, int priority) {
   void* f = pick(false, shape);
   if (!f) return (int)cudaErrorInvalidValue;
   void* args[] = {&pts, &items, &n, &chatter_idx, &out, &queue};
-  return (int)cudaLaunchKernel(f, dim3(grid), dim3(kWarp), args, (size_t)smem, stream);
+  return launch_with_priority(f, grid, smem, stream, args, priority);
 }
 
 }  // namespace mcs

@@ -1,7 +1,9 @@
 // The learned surrogate: an MLP 20 -> 256 -> 256 -> 256 -> 2 (SiLU) trained with a
 // Gaussian negative log-likelihood on log critical depths the time-domain solver
-// produced.  Weights and activations are BF16, every product accumulates in FP32
-// (mma.sync m16n8k16), the Adam state and master weights are FP32.
+// produced.  Weights and activations are BF16 and every product accumulates in FP32; the
+// Adam state and master weights are FP32.  Training (forward, backward, Adam) runs on
+// mma.sync m16n8k16 GEMMs with strided operands; inference runs in one fused kernel on
+// the 5th-generation tensor cores (tcgen05.mma with the accumulator in tensor memory).
 //
 // Layers are padded to tensor-core shapes: the 20 inputs to 32, the 2 outputs to 16;
 // padded weights start at zero and get zero gradients, so they stay zero.
@@ -234,20 +236,252 @@ __global__ void gather_rows(const float* __restrict__ X, const int32_t* __restri
   if (c == 0 && yb) yb[b] = row < n ? y[row] : 0.f;
 }
 
-// prediction -> (mu, sigma), and the guide (mu, hw) of the guided solve (hw < 0: direct)
-__global__ void predict_out(const float* __restrict__ out, int n, float* __restrict__ mu,
-                            float* __restrict__ sigma, float2* __restrict__ guide, float z,
-                            float hw_min, float hw_max, float hw_direct) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
-  const float m = out[(long)b * kOutPad];
-  const float s = expf(fminf(fmaxf(out[(long)b * kOutPad + 1], kSMin), kSMax));
-  if (mu) mu[b] = m;
-  if (sigma) sigma[b] = s;
-  if (guide) {
-    const float w = z * s;
-    guide[b] = make_float2(m, w > hw_direct ? -1.f : fminf(fmaxf(w, hw_min), hw_max));
+
+
+// ------------------------------------------------ inference on the 5th-generation tensor cores
+// One CTA of 4 warps owns a tile of 128 rows and runs all four layers on it:
+//   * the activation tile A[128 x K] (BF16) stays in shared memory, and each layer's output
+//     is written back over it as the next layer's input;
+//   * a layer's weights, kept in global memory as W^T[N x K] in the operand layout below,
+//     are copied into a shared-memory buffer (at most 256 x 256 BF16 = 128 KB);
+//   * one thread issues tcgen05.mma (M = 128, N = 256 or 16, K = 16 per instruction,
+//     kind::f16 with BF16 operands and an FP32 accumulator in tensor memory) and commits
+//     to an mbarrier;
+//   * the four warps read their 32 accumulator lanes back with tcgen05.ld, add the bias,
+//     apply SiLU and store BF16 (or, after the last layer, write mu, sigma and the guide).
+// Operand layout in shared memory (K-major, no swizzle): element (row, k) of an R-row
+// operand sits at ((k / 8) * R + row) * 8 + k % 8, so a core matrix of 8 rows x 16 bytes is
+// contiguous, 8-row groups are 128 bytes apart (stride byte offset) and the two 8-element
+// halves of one K = 16 step are R * 16 bytes apart (leading byte offset).
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 128;
+constexpr int kTcCols = 256;                          // tensor-memory columns (N <= 256)
+constexpr int kTcSmemA = kTcRows * kHid * 2;          // 64 KB
+constexpr int kTcSmemW = kHid * kHid * 2;             // 128 KB
+constexpr int kTcConst = 2 * kIn + 3 * kHid + kOutPad;  // mean, std, b0..b3 (floats)
+constexpr int kTcSmem = kTcSmemA + kTcSmemW + kTcConst * 4 + 16;
+constexpr long long kTcWaitCycles = 4000000000LL;     // ~2 s at 2 GHz: an MMA takes microseconds
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+// shared-memory matrix descriptor: start, leading and stride byte offsets (16-byte units),
+// descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major
+__host__ __device__ constexpr uint32_t instr_desc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(kTcRows >> 4) << 24);
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// bounded wait for the mbarrier phase `parity` to complete
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kTcWaitCycles) return false;
   }
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16(lo)) |
+         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16(hi)) << 16);
+}
+
+// layer shapes and bias offsets of the parameter blob, usable in device code
+__host__ __device__ constexpr int layer_k(int l) { return l == 0 ? kInPad : kHid; }
+__host__ __device__ constexpr int layer_n(int l) { return l == kLayers - 1 ? kOutPad : kHid; }
+__host__ __device__ constexpr int bias_off(int l) {
+  return l == 0 ? 2 * kIn + kInPad * kHid
+                : bias_off(l - 1) + layer_n(l - 1) + layer_k(l) * layer_n(l);
+}
+static_assert(bias_off(0) == 8232 && bias_off(3) == 144168, "parameter blob layout");
+
+struct TcWeights {
+  const bf16* w[kLayers];  // W^T of each layer in the operand layout
+};
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    mlp_infer_tc(const float* __restrict__ X, long n, const float* __restrict__ params,
+                 TcWeights tw, float* __restrict__ mu, float* __restrict__ sigma,
+                 float2* __restrict__ guide, float z, float hw_min, float hw_max,
+                 float hw_direct, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  bf16* A = reinterpret_cast<bf16*>(smem);
+  bf16* W = reinterpret_cast<bf16*>(smem + kTcSmemA);
+  float* cst = reinterpret_cast<float*>(smem + kTcSmemA + kTcSmemW);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(cst + kTcConst);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const float* mean = cst;
+  const float* stdv = cst + kIn;
+  const float* bias[kLayers] = {cst + 2 * kIn, cst + 2 * kIn + kHid, cst + 2 * kIn + 2 * kHid,
+                                cst + 2 * kIn + 3 * kHid};
+  for (int i = tid; i < 2 * kIn; i += kTcThreads) cst[i] = params[i];
+  for (int l = 0; l < kLayers; l++)
+    for (int i = tid; i < layer_n(l); i += kTcThreads)
+      cst[2 * kIn + l * kHid + i] = params[bias_off(l) + i];
+  const uint32_t bar_a = smem_addr(bar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(tmem_slot)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+  const uint32_t a_base = smem_addr(A), w_base = smem_addr(W);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (long tile = blockIdx.x; ok && tile * kTcRows < n; tile += gridDim.x) {
+    const long row = tile * kTcRows + tid;
+    // normalised features of this thread's row -> K chunks 0..3 of A (inputs 20..31 are 0)
+    {
+      float v[kInPad];
+#pragma unroll
+      for (int c = 0; c < kInPad; c++) v[c] = 0.f;
+      if (row < n) {
+#pragma unroll
+        for (int c = 0; c < kIn; c++) v[c] = (X[row * kIn + c] - mean[c]) / stdv[c];
+      }
+#pragma unroll
+      for (int kc = 0; kc < kInPad / 8; kc++) {
+        uint4 q;
+        q.x = pack_bf16(v[8 * kc + 0], v[8 * kc + 1]);
+        q.y = pack_bf16(v[8 * kc + 2], v[8 * kc + 3]);
+        q.z = pack_bf16(v[8 * kc + 4], v[8 * kc + 5]);
+        q.w = pack_bf16(v[8 * kc + 6], v[8 * kc + 7]);
+        *reinterpret_cast<uint4*>(A + ((size_t)kc * kTcRows + tid) * 8) = q;
+      }
+    }
+#pragma unroll 1
+    for (int l = 0; l < kLayers; l++) {
+      const int K = layer_k(l), N = layer_n(l);
+      {  // this layer's W^T: a contiguous copy, 16 bytes per thread and step
+        const uint4* src = reinterpret_cast<const uint4*>(tw.w[l]);
+        uint4* dst = reinterpret_cast<uint4*>(W);
+        const int nvec = K * N / 8;
+        for (int i = tid; i < nvec; i += kTcThreads) dst[i] = src[i];
+      }
+      // make the generic-proxy stores visible to the tensor core, and order the previous
+      // layer's tensor-memory reads before the new MMAs
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t idesc = instr_desc(N);
+        for (int ks = 0; ks < K / 16; ks++) {
+          const uint64_t ad = smem_desc(a_base + ks * 2 * (kTcRows * 16), kTcRows * 16, 128);
+          const uint64_t bd = smem_desc(w_base + ks * 2 * (N * 16), N * 16, 128);
+          const uint32_t acc = ks > 0 ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                bar_a)
+            : "memory");
+      }
+      ok = mbar_wait(bar_a, phase);
+      phase ^= 1u;
+      ok = __syncthreads_and(ok) != 0;  // one decision for the whole block
+      tc_fence_after();
+      if (!ok) break;
+      const float* b = bias[l];
+      if (l < kLayers - 1) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < N; c0 += 16) {
+          uint32_t r[16];
+          tmem_ld16(lane_base + (uint32_t)c0, r);
+          float h[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const float v = __uint_as_float(r[j]) + b[c0 + j];
+            h[j] = v * sigmoid(v);
+          }
+#pragma unroll
+          for (int half = 0; half < 2; half++) {
+            uint4 q;
+            q.x = pack_bf16(h[8 * half + 0], h[8 * half + 1]);
+            q.y = pack_bf16(h[8 * half + 2], h[8 * half + 3]);
+            q.z = pack_bf16(h[8 * half + 4], h[8 * half + 5]);
+            q.w = pack_bf16(h[8 * half + 6], h[8 * half + 7]);
+            *reinterpret_cast<uint4*>(A + ((size_t)(c0 / 8 + half) * kTcRows + tid) * 8) = q;
+          }
+        }
+      } else {
+        uint32_t r[16];
+        tmem_ld16(lane_base, r);
+        if (row < n) {
+          const float m = __uint_as_float(r[0]) + b[0];
+          const float sv = expf(fminf(fmaxf(__uint_as_float(r[1]) + b[1], kSMin), kSMax));
+          if (mu) mu[row] = m;
+          if (sigma) sigma[row] = sv;
+          if (guide) {
+            const float w = z * sv;
+            guide[row] = make_float2(m, w > hw_direct ? -1.f : fminf(fmaxf(w, hw_min), hw_max));
+          }
+        }
+      }
+    }
+  }
+  if (!ok) {
+    // an MMA did not complete in time: wait once more (bounded) for it before the tensor
+    // memory is released
+    mbar_wait(bar_a, phase ^ 1u);
+    if (tid == 0) atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcCols)
+                 : "memory");
+}
+
+// W[K x N] (FP32, row-major) -> BF16 W^T[N x K] in the operand layout of mlp_infer_tc
+__global__ void to_bf16_operand(const float* __restrict__ Wf, int K, int N, bf16* __restrict__ out) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)K * N) return;
+  const int k = (int)(i / N), nn = (int)(i % N);
+  out[((long)(k / 8) * N + nn) * 8 + (k % 8)] = __float2bfloat16(Wf[i]);
 }
 
 inline int blocks(long n, int t) { return (int)((n + t - 1) / t); }
@@ -271,7 +505,6 @@ struct Acts {
   bf16* dzb = nullptr;
   float* dh = nullptr;
 };
-constexpr int kInferRows = 16384;  // inference chunk; its buffers are never reallocated
 }  // namespace
 }  // namespace mcs
 
@@ -284,8 +517,10 @@ struct mcs_surrogate {
   float* m = nullptr;
   float* v = nullptr;
   bf16* Wb[kLayers] = {};
+  bf16* Wt[kLayers] = {};  // W^T in the tensor-core operand layout (inference)
+  int* err = nullptr;      // set by an inference kernel whose MMA wait timed out
+  int sms = 0;
   long step = 0;
-  Acts inf;  // inference (captured plans keep pointers into it)
   Acts tr;   // training and gradients
   float* loss = nullptr;
   std::atomic<int> plans{0};  // guided plans holding this surrogate
@@ -381,6 +616,8 @@ int cast_weights(mcs_surrogate* s, cudaStream_t st) {
   for (int l = 0; l < kLayers; l++) {
     const long n = (long)kK[l] * kN[l];
     to_bf16<<<blocks(n, 256), 256, 0, st>>>(s->params + kLay.W[l], n, s->Wb[l]);
+    to_bf16_operand<<<blocks(n, 256), 256, 0, st>>>(s->params + kLay.W[l], kK[l], kN[l],
+                                                    s->Wt[l]);
   }
   MCS_CUDA_RET(cudaGetLastError());
   return MCS_OK;
@@ -435,27 +672,42 @@ void loss_grad(mcs_surrogate* s, Acts& A, int rows, cudaStream_t st) {
 
 // ---- internal entry points used by the guided solve (mcs_api.cu) ----
 // Allocates the inference buffers once (before any stream capture that uses them).
-int surrogate_reserve(mcs_surrogate* s) { return ensure_acts(s->inf, kInferRows); }
+// Sets up what inference needs before any stream capture that uses it.
+int surrogate_reserve(mcs_surrogate* s) {
+  MCS_CUDA_RET(cudaFuncSetAttribute(mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kTcSmem));
+  return MCS_OK;
+}
 
+// mu, sigma and the guide of n rows of raw features on the device (tcgen05 kernel).  Rows
+// a timed-out kernel did not reach keep a NaN guide, which sends them to the plain
+// bisection.
 int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d_mu,
                              float* d_sigma, float2* d_guide, const mcs_guide_opts* g,
                              cudaStream_t st) {
-  const int chunk = kInferRows;
+  if (n <= 0) return MCS_OK;
   int rc = surrogate_reserve(s);
   if (rc) return rc;
-  Acts& A = s->inf;
-  for (long off = 0; off < n; off += chunk) {
-    const int rows = (int)std::min<long>(chunk, n - off);
-    gather_rows<<<blocks((long)rows * kInPad, 256), 256, 0, st>>>(
-        dX, nullptr, off, rows, n, s->params + kLay.mean, s->params + kLay.stdv, nullptr, A.xb,
-        nullptr);
-    forward(s, A, rows, st);
-    predict_out<<<blocks(rows, 256), 256, 0, st>>>(
-        A.z[kLayers - 1], rows, d_mu ? d_mu + off : nullptr, d_sigma ? d_sigma + off : nullptr,
-        d_guide ? d_guide + off : nullptr, g ? g->z : 0.f, g ? g->hw_min : 0.f,
-        g ? g->hw_max : 0.f, g ? g->hw_direct : 0.f);
-  }
+  if (d_guide) MCS_CUDA_RET(cudaMemsetAsync(d_guide, 0xFF, sizeof(float2) * n, st));
+  TcWeights tw;
+  for (int l = 0; l < kLayers; l++) tw.w[l] = s->Wt[l];
+  const long tiles = (n + kTcRows - 1) / kTcRows;
+  const int grid = (int)std::min<long>(tiles, std::max(1, s->sms));
+  mlp_infer_tc<<<grid, kTcThreads, kTcSmem, st>>>(
+      dX, n, s->params, tw, d_mu, d_sigma, d_guide, g ? g->z : 0.f, g ? g->hw_min : 0.f,
+      g ? g->hw_max : 0.f, g ? g->hw_direct : 0.f, s->err);
   MCS_CUDA_RET(cudaGetLastError());
+  return MCS_OK;
+}
+
+// Reports (and clears) a timed-out inference; call after the stream has been synchronised.
+int surrogate_check(mcs_surrogate* s) {
+  int e = 0;
+  MCS_CUDA_RET(cudaMemcpy(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    cudaMemset(s->err, 0, sizeof(int));
+    return fail(MCS_ERR_CUDA, "surrogate inference: a tensor-core wait timed out");
+  }
   return MCS_OK;
 }
 
@@ -505,10 +757,17 @@ int mcs_surrogate_create(mcs_ctx* ctx, uint64_t seed, mcs_surrogate** out) {
     return rc;
   }
   for (int l = 0; l < kLayers; l++)
-    if ((rc = dalloc(&s->Wb[l], (size_t)kK[l] * kN[l]))) {
+    if ((rc = dalloc(&s->Wb[l], (size_t)kK[l] * kN[l])) ||
+        (rc = dalloc(&s->Wt[l], (size_t)kK[l] * kN[l]))) {
       mcs_surrogate_destroy(s);
       return rc;
     }
+  if ((rc = dalloc(&s->err, 1)) || (rc = surrogate_reserve(s))) {
+    mcs_surrogate_destroy(s);
+    return rc;
+  }
+  cudaMemset(s->err, 0, sizeof(int));
+  cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, ctx_device(ctx));
   std::vector<float> p;
   init_host(p, seed);
   if ((rc = upload_params(s, p.data())) || (rc = cast_weights(s, ctx_stream(ctx))) ||
@@ -527,14 +786,17 @@ int mcs_surrogate_destroy(mcs_surrogate* s) {
     return fail(MCS_ERR_STATE, "%d guided plan(s) still use this surrogate", s->plans.load());
   cudaSetDevice(ctx_device(s->ctx));
   cudaStreamSynchronize(ctx_stream(s->ctx));
-  free_acts(s->inf);
   free_acts(s->tr);
   cudaFree(s->params);
   cudaFree(s->grad);
   cudaFree(s->m);
   cudaFree(s->v);
   cudaFree(s->loss);
-  for (int l = 0; l < kLayers; l++) cudaFree(s->Wb[l]);
+  for (int l = 0; l < kLayers; l++) {
+    cudaFree(s->Wb[l]);
+    cudaFree(s->Wt[l]);
+  }
+  cudaFree(s->err);
   delete s;
   return MCS_OK;
 }
@@ -756,6 +1018,7 @@ int mcs_surrogate_predict(mcs_surrogate* s, const float* X, size_t n, float* mu,
   cudaMemcpyAsync(dX, X, n * kIn * sizeof(float), cudaMemcpyHostToDevice, st);
   rc = surrogate_predict_device(s, dX, (long)n, dmu, dsg, nullptr, nullptr, st);
   cudaError_t e = cudaStreamSynchronize(st);
+  if (!rc && e == cudaSuccess) rc = surrogate_check(s);
   if (!rc && e == cudaSuccess) e = cudaMemcpy(mu, dmu, n * sizeof(float), cudaMemcpyDeviceToHost);
   if (!rc && e == cudaSuccess)
     e = cudaMemcpy(sigma, dsg, n * sizeof(float), cudaMemcpyDeviceToHost);

@@ -43,6 +43,34 @@ def test_forward_matches_fp64_reference(ctx, params, feats):
     s.close()
 
 
+def test_tensor_core_inference_many_tiles(ctx, params, feats):
+    """Inference runs on the tcgen05 kernel (128-row tiles, persistent CTAs).  39963 rows
+    need several tiles per CTA and end in a ragged tile; the outputs match the FP64
+    reference MLP and give the same NLL as the training forward (mma.sync kernels)."""
+    import mlp_ref as R
+    from mcs import Surrogate
+
+    _, X = feats
+    rng = np.random.default_rng(2)
+    n = 40000 - 37
+    Xb = (np.concatenate([X] * 20)[:n]
+          * (1 + 0.01 * rng.standard_normal((n, X.shape[1])))).astype(np.float32)
+    p32 = params.astype(np.float32)
+    s = Surrogate(ctx, 1)
+    s.set_params(p32)
+    mu, sg = s.predict(Xb)
+    mu_r, sg_r = R.predict(p32.astype(np.float64), Xb.astype(np.float64))
+    assert np.all(np.abs(mu - mu_r) <= 0.03 * (1 + np.abs(mu_r)))
+    assert np.all(np.abs(sg / sg_r - 1) <= 0.06)
+    y = (mu_r[:4096] + rng.normal(scale=0.3, size=4096)).astype(np.float32)
+    loss_train, _ = s.grad(Xb[:4096], y)
+    ls = np.log(sg[:4096].astype(np.float64))
+    loss_tc = float(np.mean(ls + 0.5 * (y - mu[:4096]) ** 2 * np.exp(-2 * ls)))
+    print(f"NLL: training forward {loss_train:.5f}, tensor-core inference {loss_tc:.5f}")
+    assert loss_tc == pytest.approx(loss_train, rel=2e-3, abs=2e-3)
+    s.close()
+
+
 def test_gradient_matches_fp64_reference(ctx, params, feats):
     """The gradient check of the training kernels against the CPU oracle."""
     import mlp_ref as R
