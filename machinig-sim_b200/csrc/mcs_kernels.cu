@@ -51,6 +51,19 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Fx summed over the warp into lanes 0-15 and Fy into lanes 16-31, in one butterfly: the
+// xor-16 step adds each lane's partner's share of the other half's force, the next four
+// steps reduce within each half.  Every addition has the same operands as in two separate
+// butterflies, so the sums are bit for bit those of warp_sum(Fx) and warp_sum(Fy).
+template <typename T>
+__device__ __forceinline__ T warp_sum_xy(T fx, T fy, bool upper) {
+  T v = upper ? fy : fx;
+  v += __shfl_xor_sync(kFull, upper ? fx : fy, 16);
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
 // Arithmetic of the integration scalar T (float or double).
 template <typename T>
 struct Arith;
@@ -195,22 +208,35 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   // a fresh engine's surface is all zeros (cutting.js:68)
   for (int i = lane; i < nz * lpad; i += kWarp) ring[i] = 0.f;
   __syncwarp();
+  // rounds that can hold an in-cut tooth: j = u*spt + r < len needs u < ceil(len / spt)
+  int maxlen = 0;
+#pragma unroll
+  for (int s = 0; s < SLOTS; s++) maxlen = max(maxlen, len[s]);
+  const int rounds = min(N, (__reduce_max_sync(kFull, (unsigned)maxlen) + spt - 1) / spt);
 
   // lane i < N holds tooth i's runout offset (read by shuffle)
   const T dRl = lane < kMaxTeeth ? (T)P->dR[lane] : T(0);
+  // Modal state.  Linear cuts split it: lanes 0-15 integrate the x modes and lanes 16-31
+  // the y modes (row 0 holds this half's axis), which halves the update and the force
+  // sum at the price of a broadcast of x and y on the step's critical path.  With process
+  // damping the tool velocity would need a broadcast too; there every lane integrates
+  // both axes (rows 0 and 1), which measured faster.
+  constexpr bool kSplit = !NL;
+  const bool upper = lane >= 16;
   T mk[2][NM], mcd[2][NM], ma[2][NM], q[2][NM], v[2][NM];
 #pragma unroll
   for (int a = 0; a < 2; a++)
 #pragma unroll
     for (int j = 0; j < NM; j++) {
-      mk[a][j] = (T)P->mk[a][j];
-      mcd[a][j] = (T)P->mcd[a][j];
-      ma[a][j] = (T)P->ma[a][j];
+      const int src = kSplit ? (upper ? 1 : 0) : a;
+      mk[a][j] = (T)P->mk[src][j];
+      mcd[a][j] = (T)P->mcd[src][j];
+      ma[a][j] = (T)P->ma[src][j];
       q[a][j] = T(0);
       v[a][j] = T(0);
     }
   // the kick e.vx = 0.01 m/s goes into the first x mode at the first run (cutting.js:164)
-  v[0][0] = T(0.01);
+  if (!kSplit || !upper) v[0][0] = T(0.01);
   T x = T(0), y = T(0), vxs = T(0.01), vys = T(0);
 
   const T hmax = (T)P->hmax, mc = (T)P->mc, dt = (T)P->dt;
@@ -228,7 +254,7 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     // rounds u = 0, 1, ...: in each, every lane evaluates, for each of its slots, the tooth
     // whose window offset is u*spt + r (if in cut); both slots' evaluations are
     // predicated, not branched, so their dependency chains interleave
-    for (int u = 0; u < N; u++) {
+    for (int u = 0; u < rounds; u++) {
       int jj[SLOTS];
       bool act[SLOTS];
       bool any = false;
@@ -273,27 +299,42 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
         eng += on ? 1 : 0;
       }
     }
-    Fx = warp_sum(Fx);
-    Fy = warp_sum(Fy);
     // modal integration, semi-implicit Euler; padded modes have k = c = dt/m = 0
-    T xs = T(0), ys = T(0), vxa = T(0), vya = T(0);
+    if (kSplit) {
+      // this half's force (Fx in lanes 0-15, Fy in lanes 16-31) drives this half's axis
+      const T F = warp_sum_xy(Fx, Fy, upper);
+      T qs = T(0);
 #pragma unroll
-    for (int j = 0; j < NM; j++) {
-      v[0][j] = A::madd(A::madd(-mcd[0][j], v[0][j], A::madd(-mk[0][j], q[0][j], Fx)), ma[0][j],
-                        v[0][j]);
-      q[0][j] = A::madd(v[0][j], dt, q[0][j]);
-      xs += q[0][j];
-      vxa += v[0][j];
-      v[1][j] = A::madd(A::madd(-mcd[1][j], v[1][j], A::madd(-mk[1][j], q[1][j], Fy)), ma[1][j],
-                        v[1][j]);
-      q[1][j] = A::madd(v[1][j], dt, q[1][j]);
-      ys += q[1][j];
-      vya += v[1][j];
+      for (int j = 0; j < NM; j++) {
+        v[0][j] = A::madd(A::madd(-mcd[0][j], v[0][j], A::madd(-mk[0][j], q[0][j], F)),
+                          ma[0][j], v[0][j]);
+        q[0][j] = A::madd(v[0][j], dt, q[0][j]);
+        qs += q[0][j];
+      }
+      x = __shfl_sync(kFull, qs, 0);
+      y = __shfl_sync(kFull, qs, 16);
+    } else {
+      Fx = warp_sum(Fx);
+      Fy = warp_sum(Fy);
+      T xs = T(0), ys = T(0), vxa = T(0), vya = T(0);
+#pragma unroll
+      for (int j = 0; j < NM; j++) {
+        v[0][j] = A::madd(A::madd(-mcd[0][j], v[0][j], A::madd(-mk[0][j], q[0][j], Fx)),
+                          ma[0][j], v[0][j]);
+        q[0][j] = A::madd(v[0][j], dt, q[0][j]);
+        xs += q[0][j];
+        vxa += v[0][j];
+        v[1][j] = A::madd(A::madd(-mcd[1][j], v[1][j], A::madd(-mk[1][j], q[1][j], Fy)),
+                          ma[1][j], v[1][j]);
+        q[1][j] = A::madd(v[1][j], dt, q[1][j]);
+        ys += q[1][j];
+        vya += v[1][j];
+      }
+      x = xs;
+      y = ys;
+      vxs = vxa;
+      vys = vya;
     }
-    x = xs;
-    y = ys;
-    vxs = vxa;
-    vys = vya;
     // the revolution advances one position: every slot's phase follows
 #pragma unroll
     for (int s = 0; s < SLOTS; s++) {
