@@ -175,6 +175,10 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool) -> dict:
         torch.cuda.synchronize()
         return a.elapsed_time(b), plan.results()
 
+    from mcs import tune as T
+
+    sv.opts.max_buckets, tuned = T.autotune(ctx, sv.setups, sv.modals, sv.points, sv.opts,
+                                            device_name=torch.cuda.get_device_name(device))
     with ClockSampler(device) as clk:
         pp = ctx.plan(sv.setups, sv.modals, sv.points, sv.opts)
         plain_ms, plain = run(pp)
@@ -215,6 +219,8 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool) -> dict:
         "fp64_subset": len(sub),
         "within_2pct_of_gpu_fp64": within(gres[sub], g64),
         "plain_within_2pct_of_gpu_fp64": within(plain[sub], g64),
+        "schedule": {"max_buckets": int(sv.opts.max_buckets), "tuning_ms": tuned["ms"],
+                     "from_cache": bool(tuned["cached"])},
         "model": {"file": SG.DEFAULT_MODEL.name, "epochs": rec.get("epochs"),
                   "train_points": rec.get("train_points"),
                   "val_within_15pct": rec.get("val_within_15pct")},
@@ -282,6 +288,7 @@ def ours(args) -> int:
     device = local if torch.cuda.is_available() else 0
     torch.cuda.set_device(device)
     import mcs
+    from mcs import tune as T
     from mcs import workloads as W
 
     wl = W.sweep(seed=1 + rank)
@@ -308,8 +315,13 @@ def ours(args) -> int:
         for f in ("a_min", "a_max", "iters", "revs", "nonlinear", "honor_runout",
                   "steps_per_tooth", "slices", "chatter_idx"):
             setattr(opts, f, getattr(wl.opts, f))
+        # schedule (number of shared-memory size classes) from the autotuner, untimed
+        opts.max_buckets, tuned = T.autotune(ctx, wl.setups, wl.modals, wl.points, opts,
+                                             device_name=torch.cuda.get_device_name(device))
         plan = ctx.plan(wl.setups, wl.modals, wl.points, opts)
         info = plan.info()
+        info["schedule"] = {"max_buckets": int(opts.max_buckets), "tuning_ms": tuned["ms"],
+                            "from_cache": bool(tuned["cached"])}
         for _ in range(args.warmup):
             plan.execute()
         res = plan.results()
@@ -412,7 +424,8 @@ def ours(args) -> int:
                                   "modal integration, FP64 statistics and bracket",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "kernels_per_step": info["kernels"], "graph": bool(info["graph"]),
-                       "blocks": info["blocks"], "smem_per_warp_max": info["smem_per_warp"]},
+                       "blocks": info["blocks"], "smem_per_warp_max": info["smem_per_warp"],
+                       "schedule": info["schedule"]},
             "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops,
                          "unit": "TFLOP/s", "frac": achieved_tflops / peak_tflops,
                          "traffic": None,

@@ -115,8 +115,12 @@ typedef struct {
   int32_t slices;          /* 0: reference rule dz = max(0.25, fluteLen/48) */
   double chatter_idx;      /* decision threshold (reference 0.45, stabtd.js:10) */
   int32_t precision;       /* mcs_precision of the force law and modal integration */
-  int32_t pad;
+  int32_t max_buckets;     /* schedule: at most this many shared-memory size classes, each
+                              its own persistent grid (1..MCS_MAX_BUCKETS; 0: 16); results
+                              do not depend on it, only the time does (see mcs_tune) */
 } mcs_opts;
+
+#define MCS_MAX_BUCKETS 32
 
 /* Result of timeDomainLimit for one point. */
 typedef struct {
@@ -253,6 +257,19 @@ void mcs_job_free(mcs_job* job);
 int mcs_solve_noalloc(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,
                       const mcs_modal* modals, size_t n_modals, const mcs_point* points,
                       size_t n_points, const mcs_opts* opts, mcs_result* out);
+
+/* ------------------------------------------------------------------ schedule tuning
+ * The autotuner of the schedule: no counterpart in the reference.  It captures a plan of
+ * the batch for every candidate max_buckets (at most 64 candidates), runs each once
+ * untimed, then times three round-robin rounds of one execution per candidate, each after
+ * a write of twice the L2 size (so from a cold L2; the tuner allocates that buffer).  ms[]
+ * (NULL allowed) receives each candidate's fastest round and *best the fastest candidate.
+ * opts->max_buckets is ignored.  Results of a solve are identical for every schedule; only
+ * the time changes.
+ */
+int mcs_tune(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+             size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* opts,
+             const int32_t* candidates, size_t n_candidates, double* ms, int32_t* best);
 
 /* ------------------------------------------------------------------ surrogate
  * A small MLP (20 -> 256 -> 256 -> 256 -> 2, SiLU, BF16 weights and activations with FP32

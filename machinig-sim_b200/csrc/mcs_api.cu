@@ -42,7 +42,8 @@ namespace {
   } while (0)
 
 constexpr double kPi = 3.141592653589793;
-constexpr int kMaxBuckets = 8;
+constexpr int kMaxBuckets = MCS_MAX_BUCKETS;
+constexpr int kDefaultBuckets = 16;
 
 inline bool is_finite(double v) { return std::isfinite(v); }
 
@@ -67,6 +68,8 @@ int check_inputs(const mcs_setup* setups, size_t n_setups, const mcs_modal* moda
   if (!is_finite(o->chatter_idx)) return fail(MCS_ERR_ARG, "chatter_idx is not finite");
   if (o->precision != MCS_FP32 && o->precision != MCS_FP64)
     return fail(MCS_ERR_ARG, "precision must be MCS_FP32 or MCS_FP64");
+  if (o->max_buckets < 0 || o->max_buckets > kMaxBuckets)
+    return fail(MCS_ERR_ARG, "max_buckets out of range [0, %d]", kMaxBuckets);
   for (size_t i = 0; i < n_setups; i++) {
     const mcs_setup& s = setups[i];
     const mcs_tool& t = s.tool;
@@ -372,8 +375,9 @@ namespace {
 // shared-memory need, each launched as its own persistent grid.
 int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
                  const std::vector<int>& slots, const std::vector<int>& modes,
-                 const std::vector<int>& nls, bool trials, int fp64,
+                 const std::vector<int>& nls, bool trials, int fp64, int max_buckets,
                  std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
+  const int nbmax = max_buckets > 0 ? std::min(max_buckets, kMaxBuckets) : kDefaultBuckets;
   const size_t n = smem.size();
   std::vector<int32_t> idx(n);
   std::iota(idx.begin(), idx.end(), 0);
@@ -383,7 +387,8 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
   order.reserve(n);
   if (n == 0) return MCS_OK;
   const double hi = smem[idx.front()], lo = std::max(1, smem[idx.back()]);
-  const double ratio = std::max(1.3, std::pow(hi / lo, 1.0 / kMaxBuckets) * 1.0001);
+  // size classes: a bucket holds the points within a factor `ratio` of its largest need
+  const double ratio = std::max(1.1, std::pow(hi / lo, 1.0 / nbmax) * 1.0001);
   size_t i = 0;
   while (i < n) {
     Bucket b;
@@ -396,7 +401,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
       nl = std::max(nl, nls[idx[j]]);
       j++;
     }
-    if ((int)buckets.size() == kMaxBuckets - 1) {  // last bucket takes the rest
+    if ((int)buckets.size() == nbmax - 1) {  // last bucket takes the rest
       for (size_t k = j; k < n; k++) {
         sl = std::max(sl, slots[idx[k]]);
         nm = std::max(nm, modes[idx[k]]);
@@ -576,7 +581,8 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
-  rc = make_buckets(ctx, smem, cost, slots, modes, nls, false, o->precision == MCS_FP64, order,
+  rc = make_buckets(ctx, smem, cost, slots, modes, nls, false, o->precision == MCS_FP64,
+                    o->max_buckets, order,
                     pl->buckets);
   if (rc) {
     plan_free(pl);
@@ -668,7 +674,7 @@ void mcs_default_opts(mcs_opts* o) {
   o->slices = 0;
   o->chatter_idx = 0.45;
   o->precision = MCS_FP32;
-  o->pad = 0;
+  o->max_buckets = 0;
 }
 
 const char* mcs_last_error(void) { return g_last_error.c_str(); }
@@ -794,6 +800,81 @@ int mcs_plan_destroy(mcs_plan* pl) {
   return MCS_OK;
 }
 
+int mcs_tune(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+             size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* opts,
+             const int32_t* candidates, size_t n_candidates, double* ms, int32_t* best) {
+  if (!c || !opts || !best) return fail(MCS_ERR_ARG, "NULL ctx, opts or best");
+  if (n_candidates == 0 || !candidates) return fail(MCS_ERR_ARG, "no candidate schedules");
+  if (n_candidates > 64) return fail(MCS_ERR_ARG, "at most 64 candidate schedules");
+  for (size_t i = 0; i < n_candidates; i++)
+    if (candidates[i] < 1 || candidates[i] > kMaxBuckets)
+      return fail(MCS_ERR_ARG, "candidate %zu: max_buckets %d out of range [1, %d]", i,
+                  candidates[i], kMaxBuckets);
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  // all candidate plans first; then kRounds rounds in which every candidate runs once,
+  // round-robin, so that a drift of the clocks does not favour one candidate; each
+  // candidate's time is its fastest round
+  constexpr int kRounds = 3;
+  std::vector<mcs_plan*> plans(n_candidates, nullptr);
+  std::vector<double> t(n_candidates, INFINITY);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = MCS_OK;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    rc = fail(MCS_ERR_CUDA, "event creation failed");
+  // every timed run starts from a cold L2, as after unrelated work: a schedule measured
+  // back to back on a warm L2 ranked differently (24 classes: 200 ms warm, 250-300 ms cold)
+  int l2 = 0;
+  cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device);
+  const size_t flush_bytes = 2 * (size_t)std::max(l2, 1 << 20);
+  void* flush = nullptr;
+  if (!rc && cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
+    flush = nullptr;
+    rc = fail(MCS_ERR_NOMEM, "no room for the L2 flush buffer (%zu bytes)", flush_bytes);
+  }
+  for (size_t i = 0; i < n_candidates && !rc; i++) {
+    mcs_opts o = *opts;
+    o.max_buckets = candidates[i];
+    rc = build_plan(c, setups, n_setups, modals, n_modals, points, n_points, &o, true, c->stream,
+                    &plans[i]);
+  }
+  cudaError_t e = cudaSuccess;
+  for (int r = -1; r < kRounds && !rc && e == cudaSuccess; r++) {
+    for (size_t i = 0; i < n_candidates && e == cudaSuccess; i++) {
+      if (!plans[i]->exec) {
+        t[i] = 0.0;
+        continue;
+      }
+      if (r < 0) {  // untimed: the first launch uploads the graph
+        e = cudaGraphLaunch(plans[i]->exec, c->stream);
+        continue;
+      }
+      float f = 0.f;
+      e = cudaMemsetAsync(flush, (r * 31 + (int)i) & 0xFF, flush_bytes, c->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+      if (e == cudaSuccess) e = cudaGraphLaunch(plans[i]->exec, c->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+      if (e == cudaSuccess) t[i] = std::min(t[i], (double)f);
+    }
+  }
+  cudaStreamSynchronize(c->stream);
+  for (mcs_plan* pl : plans) plan_free(pl);
+  if (flush) cudaFree(flush);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "tuning run failed: %s", cudaGetErrorString(e));
+  if (rc) return rc;
+  size_t bi = 0;
+  for (size_t i = 0; i < n_candidates; i++) {
+    if (ms) ms[i] = t[i];
+    if (t[i] < t[bi]) bi = i;
+  }
+  *best = candidates[bi];
+  return MCS_OK;
+}
+
 int mcs_solve(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
               size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* opts,
               mcs_result* out) {
@@ -870,7 +951,8 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
   pl->trials = true;
   pl->n = n_trials;
   std::vector<int32_t> order;
-  rc = make_buckets(c, smem, cost, slots, tmodes, tnl, true, o->precision == MCS_FP64, order,
+  rc = make_buckets(c, smem, cost, slots, tmodes, tnl, true, o->precision == MCS_FP64,
+                    o->max_buckets, order,
                     pl->buckets);
   std::vector<TrialItem> items(n_trials);
   for (size_t k = 0; k < order.size(); k++) items[k] = items_by_idx[order[k]];

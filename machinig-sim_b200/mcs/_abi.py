@@ -82,7 +82,8 @@ class Opts(C.Structure):
     _fields_ = [("a_min", C.c_double), ("a_max", C.c_double), ("iters", C.c_int32),
                 ("revs", C.c_int32), ("nonlinear", C.c_int32), ("honor_runout", C.c_int32),
                 ("steps_per_tooth", C.c_int32), ("slices", C.c_int32),
-                ("chatter_idx", C.c_double), ("precision", C.c_int32), ("pad", C.c_int32)]
+                ("chatter_idx", C.c_double), ("precision", C.c_int32),
+                ("max_buckets", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -176,8 +177,9 @@ def make_setup(tool, mat, arc: Sequence[float], fz: float) -> Setup:
 
 def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
     """timeDomainLimit/chatterAt options (src/stabtd.js:14,24) with the reference defaults,
-    plus the explicit extensions honorRunout, stepsPerTooth, slices, chatterIdx and
-    precision ("fp32": FP32 force law and modal integration, "fp64": FP64)."""
+    plus the explicit extensions honorRunout, stepsPerTooth, slices, chatterIdx,
+    precision ("fp32": FP32 force law and modal integration, "fp64": FP64) and maxBuckets
+    (the schedule; 0 = the library's default, see mcs.tune)."""
     d = dict(DEFAULTS)
     if o:
         d.update(o)
@@ -186,11 +188,13 @@ def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
                 1 if d.get("nonlinear", True) is not False else 0,
                 1 if d.get("honorRunout", False) else 0,
                 int(d.get("stepsPerTooth", 0) or 0), int(d.get("slices", 0) or 0),
-                float(d.get("chatterIdx", CHATTER_IDX)), precision_code(d.get("precision")), 0)
+                float(d.get("chatterIdx", CHATTER_IDX)), precision_code(d.get("precision")),
+                int(d.get("maxBuckets", 0) or 0))
 
 
 FP32 = 0
 FP64 = 1
+MAX_BUCKETS = 32
 
 
 def precision_code(p) -> int:
@@ -253,7 +257,7 @@ TRIAL_DTYPE = np.dtype([("point", "<u4"), ("pad", "<u4"), ("ap", "<f8")])
 OPTS_DTYPE = np.dtype([("a_min", "<f8"), ("a_max", "<f8"), ("iters", "<i4"), ("revs", "<i4"),
                        ("nonlinear", "<i4"), ("honor_runout", "<i4"),
                        ("steps_per_tooth", "<i4"), ("slices", "<i4"), ("chatter_idx", "<f8"),
-                       ("precision", "<i4"), ("pad", "<i4")])
+                       ("precision", "<i4"), ("max_buckets", "<i4")])
 for _d, _c in ((MODAL_DTYPE, Modal), (SETUP_DTYPE, Setup), (POINT_DTYPE, Point),
                (TRIAL_DTYPE, Trial), (OPTS_DTYPE, Opts)):
     assert _d.itemsize == C.sizeof(_c), (_d, _c)

@@ -27,7 +27,7 @@ EXPORTS = (
     "mcs_default_train_opts", "mcs_default_guide_opts", "mcs_features", "mcs_surrogate_create",
     "mcs_surrogate_destroy", "mcs_surrogate_train", "mcs_surrogate_predict", "mcs_surrogate_grad",
     "mcs_surrogate_get_params", "mcs_surrogate_set_params", "mcs_solve_guided",
-    "mcs_plan_create_guided", "mcs_plan_guide_info",
+    "mcs_plan_create_guided", "mcs_plan_guide_info", "mcs_tune",
 )
 _VOID = ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free",
          "mcs_default_train_opts", "mcs_default_guide_opts")
@@ -79,6 +79,7 @@ def load(path: Path | str | None = None):
         L.mcs_job_free.argtypes = [vp]
         L.mcs_job_free.restype = None
         L.mcs_lobes_alim.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, vp]
+        L.mcs_tune.argtypes = batch + [vp, C.c_size_t, vp, P(C.c_int32)]
         L.mcs_solve_noalloc.argtypes = batch + [vp]
         L.mcs_default_train_opts.argtypes = [P(A.TrainOpts)]
         L.mcs_default_train_opts.restype = None
@@ -283,6 +284,16 @@ class Context:
         check(self._L.mcs_solve_guided(self._h, surrogate._h, *b.args(), C.byref(opts),
                                        C.byref(g), _ptr(out), _ptr(info)))
         return out[:n], info[:n]
+
+    def tune(self, setups, modals, points, opts: A.Opts, candidates=(4, 8, 16, 32)):
+        """(best max_buckets, {candidate: ms}) from one timed execution per candidate."""
+        b = Batch(setups, modals, points)
+        cand = np.ascontiguousarray(candidates, dtype=np.int32)
+        ms = np.zeros(len(cand), dtype=np.float64)
+        best = C.c_int32()
+        check(self._L.mcs_tune(self._h, *b.args(), C.byref(opts), _ptr(cand), len(cand),
+                               _ptr(ms), C.byref(best)))
+        return int(best.value), {int(c): float(t) for c, t in zip(cand, ms)}
 
     def solve_async(self, setups, modals, points, opts: A.Opts) -> Job:
         return Job(self, Batch(setups, modals, points), opts)

@@ -1,0 +1,64 @@
+"""The schedule autotuner on the GPU: results do not depend on the schedule, the tuner
+times every candidate and picks one of them, and a cached choice is reused."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_results_identical_for_every_schedule(ctx):
+    from mcs import _abi as A
+    from mcs import workloads as W
+
+    wl = W.hetero(n=1536, first_seed=777)
+    ref = None
+    for nb in (1, 3, 16, 32):
+        o = A.make_opts(dict(W.HETERO_OPTS), maxBuckets=nb)
+        r = ctx.solve(wl.setups, wl.modals, wl.points, o)
+        plan = ctx.plan(wl.setups, wl.modals, wl.points, o)
+        plan.execute()
+        assert plan.results().tobytes() == r.tobytes()
+        assert plan.info()["kernels"] <= nb
+        plan.close()
+        if ref is None:
+            ref = r
+        assert r.tobytes() == ref.tobytes(), nb
+
+
+def test_tune_times_every_candidate(ctx):
+    from mcs import workloads as W
+
+    wl = W.sweep(n_speeds=512)
+    best, ms = ctx.tune(wl.setups, wl.modals, wl.points, wl.opts, (2, 8, 16))
+    assert best in (2, 8, 16)
+    assert set(ms) == {2, 8, 16} and all(v > 0 for v in ms.values())
+    assert ms[best] == min(ms.values())
+
+
+def test_tune_rejects_bad_schedules(ctx):
+    from mcs import MCSError, _abi as A
+    from mcs import workloads as W
+
+    wl = W.sweep(n_speeds=64)
+    for bad in ((0,), (33,), ()):
+        with pytest.raises(MCSError):
+            ctx.tune(wl.setups, wl.modals, wl.points, wl.opts, bad)
+    o = A.make_opts(maxBuckets=A.MAX_BUCKETS + 1)
+    with pytest.raises(MCSError):
+        ctx.solve(wl.setups, wl.modals, wl.points, o)
+
+
+def test_autotune_caches_its_choice(ctx, tmp_path):
+    from mcs import tune as T
+    from mcs import workloads as W
+
+    wl = W.hetero(n=1024, first_seed=4242)
+    path = tmp_path / "tune.json"
+    best, rec = T.autotune(ctx, wl.setups, wl.modals, wl.points, wl.opts, candidates=(4, 16),
+                           sample=512, cache=path)
+    assert not rec["cached"] and rec["sample_points"] == 512 and best in (4, 16)
+    best2, rec2 = T.autotune(ctx, wl.setups, wl.modals, wl.points, wl.opts,
+                             candidates=(4, 16), cache=path)
+    assert rec2["cached"] and best2 == best
