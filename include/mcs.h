@@ -118,6 +118,11 @@ typedef struct {
   int32_t max_buckets;     /* schedule: at most this many shared-memory size classes, each
                               its own persistent grid (1..MCS_MAX_BUCKETS; 0: 16); results
                               do not depend on it, only the time does (see mcs_tune) */
+  int32_t serial_trials;   /* 0: a bisection runs the trials of its next levels together in
+                              lane groups of one warp when their slice counts allow
+                              (speculatively; only the trials on the decision path count);
+                              1: one trial at a time.  Results are identical either way. */
+  int32_t pad;
 } mcs_opts;
 
 #define MCS_MAX_BUCKETS 32

@@ -70,6 +70,8 @@ int check_inputs(const mcs_setup* setups, size_t n_setups, const mcs_modal* moda
     return fail(MCS_ERR_ARG, "precision must be MCS_FP32 or MCS_FP64");
   if (o->max_buckets < 0 || o->max_buckets > kMaxBuckets)
     return fail(MCS_ERR_ARG, "max_buckets out of range [0, %d]", kMaxBuckets);
+  if (o->serial_trials != 0 && o->serial_trials != 1)
+    return fail(MCS_ERR_ARG, "serial_trials must be 0 or 1");
   for (size_t i = 0; i < n_setups; i++) {
     const mcs_setup& s = setups[i];
     const mcs_tool& t = s.tool;
@@ -230,8 +232,12 @@ int prepare_point(const mcs_setup& st, const mcs_modal& md, double S_in, const m
   const long long H = (long long)P.nsteps / P.decim;
   P.hist_m = (int)std::min<long long>(H, (long long)std::floor((double)P.ts_n * spt / P.decim + 0.5));
   P.hist_h0 = (int)(H - P.hist_m);
-  const long long smem = (long long)table_bytes(P.spr, o.precision == MCS_FP64) +
-                         4LL * P.nz_max * P.lpad;
+  // trials of one point can share a warp in lane groups when their slice counts vary with
+  // depth (the reference slice rule) or are small; the ring then has a row per lane
+  P.groups = (!o.serial_trials && (o.slices == 0 || o.slices <= 16)) ? kMaxGroups : 1;
+  P.ring_rows = P.groups > 1 ? std::max(P.nz_max, kWarp) : P.nz_max;
+  const long long smem =
+      warp_smem(P.spr, o.precision == MCS_FP64, P.ring_rows, P.lpad, P.groups);
   if (smem > kMaxSmemPerWarp)
     return fail(MCS_ERR_UNSUPPORTED,
                 "point needs %lld bytes of shared memory (spr %d, %d slices): above %d", smem,
@@ -375,7 +381,8 @@ namespace {
 // shared-memory need, each launched as its own persistent grid.
 int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
                  const std::vector<int>& slots, const std::vector<int>& modes,
-                 const std::vector<int>& nls, bool trials, int fp64, int max_buckets,
+                 const std::vector<int>& nls, const std::vector<int>& grps, bool trials,
+                 int fp64, int max_buckets,
                  std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
   const int nbmax = max_buckets > 0 ? std::min(max_buckets, kMaxBuckets) : kDefaultBuckets;
   const size_t n = smem.size();
@@ -394,11 +401,12 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     Bucket b;
     const int top = smem[idx[i]];
     size_t j = i;
-    int sl = 1, nm = 1, nl = 0;
+    int sl = 1, nm = 1, nl = 0, gr = 0;
     while (j < n && (double)smem[idx[j]] * ratio >= top) {
       sl = std::max(sl, slots[idx[j]]);
       nm = std::max(nm, modes[idx[j]]);
       nl = std::max(nl, nls[idx[j]]);
+      gr = std::max(gr, grps[idx[j]]);
       j++;
     }
     if ((int)buckets.size() == nbmax - 1) {  // last bucket takes the rest
@@ -406,6 +414,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
         sl = std::max(sl, slots[idx[k]]);
         nm = std::max(nm, modes[idx[k]]);
         nl = std::max(nl, nls[idx[k]]);
+        gr = std::max(gr, grps[idx[k]]);
       }
       j = n;
     }
@@ -414,7 +423,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     b.offset = (int)order.size();
     b.count = (int)seg.size();
     b.smem = (top + 15) & ~15;
-    b.shape = KernelShape{sl, nm, fp64, nl};
+    b.shape = KernelShape{sl, nm, fp64, nl, trials ? 0 : gr};
     order.insert(order.end(), seg.begin(), seg.end());
     int bps = 0;
     const int rc = trials ? occupancy_trials(b.shape, b.smem, &bps)
@@ -563,7 +572,8 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
               !(g->hw_direct > 0) || g->refine < 0 || g->refine > 30))
     return fail(MCS_ERR_ARG, "guide options out of range");
   std::vector<PointParams> pp(n_points);
-  std::vector<int> smem(n_points), slots(n_points), modes(n_points), nls(n_points);
+  std::vector<int> smem(n_points), slots(n_points), modes(n_points), nls(n_points),
+      grps(n_points);
   std::vector<double> cost(n_points);
   for (size_t i = 0; i < n_points; i++) {
     Prepared pr;
@@ -575,13 +585,14 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
     slots[i] = slots_for(pr.pp.nz_max);
     modes[i] = pr.modes;
     nls[i] = pr.nl;
+    grps[i] = pr.pp.groups > 1 ? 1 : 0;
     cost[i] = pr.cost;
   }
   mcs_plan* pl = new mcs_plan();
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
-  rc = make_buckets(ctx, smem, cost, slots, modes, nls, false, o->precision == MCS_FP64,
+  rc = make_buckets(ctx, smem, cost, slots, modes, nls, grps, false, o->precision == MCS_FP64,
                     o->max_buckets, order,
                     pl->buckets);
   if (rc) {
@@ -675,6 +686,8 @@ void mcs_default_opts(mcs_opts* o) {
   o->chatter_idx = 0.45;
   o->precision = MCS_FP32;
   o->max_buckets = 0;
+  o->serial_trials = 0;
+  o->pad = 0;
 }
 
 const char* mcs_last_error(void) { return g_last_error.c_str(); }
@@ -939,7 +952,7 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
   for (size_t i = 0; i < n_trials; i++) {
     const PointParams& P = pp[trials[i].point];
     const int nz = slices_at(trials[i].ap, P.flute_len, o->slices);
-    smem[i] = table_bytes(P.spr, o->precision == MCS_FP64) + 4 * nz * P.lpad;
+    smem[i] = warp_smem(P.spr, o->precision == MCS_FP64, nz, P.lpad, 1);
     slots[i] = slots_for(nz);
     tmodes[i] = modes[trials[i].point];
     tnl[i] = pnl[trials[i].point];
@@ -951,7 +964,8 @@ int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,
   pl->trials = true;
   pl->n = n_trials;
   std::vector<int32_t> order;
-  rc = make_buckets(c, smem, cost, slots, tmodes, tnl, true, o->precision == MCS_FP64,
+  rc = make_buckets(c, smem, cost, slots, tmodes, tnl, std::vector<int>(n_trials, 0), true,
+                    o->precision == MCS_FP64,
                     o->max_buckets, order,
                     pl->buckets);
   std::vector<TrialItem> items(n_trials);
@@ -1280,7 +1294,7 @@ extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_s
   PointParams chunk[kNaChunk];
   double cost[kNaMax];
   int32_t order[kNaMax];
-  int smem = 0, slots = 1, modes = 1, nl = 0;
+  int smem = 0, slots = 1, modes = 1, nl = 0, gr = 0;
   for (size_t i0 = 0; i0 < n_points; i0 += kNaChunk) {
     const size_t m = std::min<size_t>(kNaChunk, n_points - i0);
     for (size_t j = 0; j < m; j++) {
@@ -1295,6 +1309,7 @@ extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_s
       slots = std::max(slots, slots_for(pr.pp.nz_max));
       modes = std::max(modes, pr.modes);
       nl = std::max(nl, pr.nl);
+      gr = std::max(gr, pr.pp.groups > 1 ? 1 : 0);
     }
     MCS_CUDA(cudaMemcpyAsync(d_params + i0, chunk, sizeof(PointParams) * m,
                              cudaMemcpyHostToDevice, st));
@@ -1307,7 +1322,7 @@ extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_s
                            st));
   // the queue counter must start at zero; the area keeps the previous call's contents
   MCS_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
-  const KernelShape shape{slots, modes, o->precision == MCS_FP64 ? 1 : 0, nl};
+  const KernelShape shape{slots, modes, o->precision == MCS_FP64 ? 1 : 0, nl, gr};
   smem = (smem + 15) & ~15;
   int bps = 0;
   const int orc = occupancy_solve(shape, smem, &bps);

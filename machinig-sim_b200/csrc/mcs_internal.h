@@ -61,8 +61,10 @@ struct alignas(16) PointParams {
   int32_t ts_n;                         // tooth samples in the window (<= 24)
   int32_t hist_h0;                      // first history sample inside the window
   int32_t hist_m;                       // history samples in the window
-  int32_t smem_bytes;                   // table + ring for the deepest trial
+  int32_t smem_bytes;                   // table + ring + sample/result area (warp_smem)
   int32_t empty;                        // arc covers no bin
+  int32_t ring_rows;                    // ring rows: nz_max, or 32 if larger and groups > 1
+  int32_t groups;                       // trials one warp may run together (1 or kMaxGroups)
 };
 
 // Shared memory of one warp: the sin/cos table of the revolution's positions (float2 or
@@ -70,6 +72,20 @@ struct alignas(16) PointParams {
 // reference stores the surface in a Float32Array).
 __host__ __device__ inline int table_bytes(int spr, bool fp64) {
   return (spr * (fp64 ? 16 : 8) + 15) & ~15;
+}
+
+// After the table and the ring: per trial group, its once-per-tooth samples (float2) and
+// its result record.  A warp runs up to kMaxGroups trials of one point together in lane
+// groups (speculative bisection levels).
+constexpr int kMaxGroups = 8;
+constexpr int kToothSamples = 24;
+constexpr int kTrialOutBytes = 48;
+__host__ __device__ inline int extra_offset(int spr, bool fp64, int ring_rows, int lpad) {
+  return (table_bytes(spr, fp64) + 4 * ring_rows * lpad + 15) & ~15;
+}
+__host__ __device__ inline int warp_smem(int spr, bool fp64, int ring_rows, int lpad,
+                                         int groups) {
+  return extra_offset(spr, fp64, ring_rows, lpad) + groups * (kToothSamples * 8 + kTrialOutBytes);
 }
 
 // Options the kernels read (mcs_opts reduced to what the device needs).
@@ -100,6 +116,7 @@ struct KernelShape {
   int modes;  // 1..4
   int fp64;   // 0: FP32 force law and modal integration, 1: FP64
   int nl;     // 1: size effect and/or process damping present
+  int grouped = 0;  // 1: points may run several trials per warp in lane groups
 };
 
 // Host launchers (mcs_kernels.cu).

@@ -111,6 +111,7 @@ struct TrialOut {
   unsigned long long engaged, evals;
   int status;
 };
+static_assert(sizeof(TrialOut) == kTrialOutBytes, "shared-memory result record");
 
 // sin/cos of every position of one revolution: theta(p) = p * dphi.
 template <typename T>
@@ -126,20 +127,10 @@ __device__ __forceinline__ void build_table(const PointParams* __restrict__ P,
   __syncwarp();
 }
 
-// One chatterAt trial at depth ap: configure + setEngagement + kick + run + chatterIndex.
-// NL: size effect and process damping present (cutting.js:153-156,197,203); linear cuts
-// are compiled without them.
-template <typename T, int SLOTS, int NM, bool NL>
-__device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
-                                   const typename Arith<T>::V2* __restrict__ table,
-                                   float* __restrict__ ring, int lane) {
-  using A = Arith<T>;
-  TrialOut res;
-  const int N = P->N, spt = P->spt, spr = P->spr, lpad = P->lpad;
-
-  // ---- slices of this trial (stabtd.js:16-18 -> cutting.js:63-64, 98-124), FP64 ----
-  int nz;
-  double dz;
+// Slices of a trial at depth ap (stabtd.js:16-18 -> cutting.js:63-64, 98-124), FP64; the
+// same rule as the host's slices_at.
+__device__ __forceinline__ void slice_rule(const PointParams* __restrict__ P, double ap,
+                                           int& nz, double& dz) {
   if (P->slices_override > 0) {
     nz = ap > 0 ? P->slices_override : 0;
     dz = ap / P->slices_override;
@@ -149,6 +140,85 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     const int maxs = (int)ceil(flute / dz);
     nz = ap > 0 ? min(maxs, (int)ceil(ap / dz)) : 0;
   }
+}
+
+// Sum over an aligned group of gs lanes (gs a power of two).  Every lane executes the same
+// five shuffles whatever its group's size (a shuffle must be reached by the whole warp); a
+// lane adds what it receives only from inside its group.  With gs = 32 it is the warp
+// butterfly; for a smaller group it adds in the same order as a whole warp would if the
+// group's values sat at lanes 0..gs-1 and the others held 0.
+template <typename T>
+__device__ __forceinline__ T group_sum(T v, int gs) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T t = __shfl_xor_sync(kFull, v, o);
+    if (o < gs) v += t;
+  }
+  return v;
+}
+__device__ __forceinline__ int group_sum_int(int v, int gs) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const int t = __shfl_xor_sync(kFull, v, o);
+    if (o < gs) v += t;
+  }
+  return v;
+}
+// Fx summed into the group's lower half and Fy into its upper half, in one butterfly (the
+// additions of group_sum(Fx) and group_sum(Fy), so the sums are bit for bit theirs).  The
+// first shuffle reads the partner in the other half of the lane's own group (a per-lane
+// source lane); the others are the same for every lane, as above.
+template <typename T>
+__device__ __forceinline__ T group_sum_xy(T fx, T fy, bool upper, int gs, int lane) {
+  T v = upper ? fy : fx;
+  v += __shfl_sync(kFull, upper ? fx : fy, lane ^ (gs >> 1));
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    const T t = __shfl_xor_sync(kFull, v, o);
+    if (o < (gs >> 1)) v += t;
+  }
+  return v;
+}
+
+// The lane groups of one warp and the depth each simulates.  Groups are aligned blocks of
+// a power-of-two number of lanes (>= 4) that cover the warp; a group with ap = 0 has no
+// slices and its result is not used.
+struct Groups {
+  int n;                    // groups
+  int base[kMaxGroups];     // first lane
+  int size[kMaxGroups];     // lanes
+  double ap[kMaxGroups];    // depth [mm]
+};
+
+// chatterAt trials (configure + setEngagement + kick + run + chatterIndex) of one point,
+// one per lane group, all stepping together: the run() loop of cutting.js:146-296 in each
+// group.  A group of g lanes with at most g * SLOTS slices computes exactly what a whole
+// warp computes for that trial.  Results go to out[group] (shared memory); tooth samples
+// are staged in samples[group][24].
+// NL: size effect and process damping present (cutting.js:153-156,197,203); linear cuts
+// are compiled without them.
+// GR: lane groups in use; without them the single group of 32 lanes is compiled as such.
+template <typename T, int SLOTS, int NM, bool NL, bool GR>
+__device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
+                         const typename Arith<T>::V2* __restrict__ table,
+                         float* __restrict__ ring, float2* __restrict__ samples,
+                         TrialOut* __restrict__ out, int lane) {
+  using A = Arith<T>;
+  const int N = P->N, spt = P->spt, spr = P->spr, lpad = P->lpad;
+  // this lane's group
+  int gi = 0;
+  if (GR) {
+#pragma unroll
+    for (int g = 1; g < kMaxGroups; g++)
+      if (g < G.n && lane >= G.base[g] && lane < G.base[g] + G.size[g]) gi = g;
+  }
+  const int gb = GR ? G.base[gi] : 0, gs = GR ? G.size[gi] : kWarp, ll = lane - gb;
+  const double ap = GR ? G.ap[gi] : G.ap[0];
+
+  // ---- slices of this trial (stabtd.js:16-18 -> cutting.js:63-64, 98-124), FP64 ----
+  int nz;
+  double dz;
+  slice_rule(P, ap, nz, dz);
   // process damping per slice, Ci*b/V_c (cutting.js:155-156,203)
   const double pdK = NL && P->Ci != 0.0 ? P->Ci * dz * 1e-3 / (P->omega * 1e-3) : 0.0;
 
@@ -162,11 +232,11 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   int p0[SLOTS], len[SLOTS], base[SLOTS], cph[SLOTS], rph[SLOTS];
 #pragma unroll
   for (int s = 0; s < SLOTS; s++) {
-    const int k = lane + kWarp * s;
+    const int k = ll + gs * s;  // slice; its ring row is the lane's own
     sL[s] = cL[s] = ktb[s] = kteb[s] = krb[s] = kreb[s] = pdc[s] = fzk[s] = T(0);
     p0[s] = 0;
     len[s] = 0;
-    base[s] = k * lpad;
+    base[s] = (gb + k) * lpad;
     if (k < nz && !P->empty) {
       const double b = fmin(dz, ap - k * dz);
       const double zr = k * dz + 0.5 * b;
@@ -205,8 +275,15 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     cph[s] = q / spt;
     rph[s] = q - cph[s] * spt;
   }
-  // a fresh engine's surface is all zeros (cutting.js:68)
-  for (int i = lane; i < nz * lpad; i += kWarp) ring[i] = 0.f;
+  // a fresh engine's surface is all zeros (cutting.js:68): the trial's rows
+  if (GR) {
+#pragma unroll
+    for (int s = 0; s < SLOTS; s++)
+      if (ll + gs * s < nz)
+        for (int j = 0; j < lpad; j++) ring[base[s] + j] = 0.f;
+  } else {
+    for (int i = lane; i < nz * lpad; i += kWarp) ring[i] = 0.f;
+  }
   __syncwarp();
   // rounds that can hold an in-cut tooth: j = u*spt + r < len needs u < ceil(len / spt)
   int maxlen = 0;
@@ -216,13 +293,13 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
 
   // lane i < N holds tooth i's runout offset (read by shuffle)
   const T dRl = lane < kMaxTeeth ? (T)P->dR[lane] : T(0);
-  // Modal state.  Linear cuts split it: lanes 0-15 integrate the x modes and lanes 16-31
-  // the y modes (row 0 holds this half's axis), which halves the update and the force
-  // sum at the price of a broadcast of x and y on the step's critical path.  With process
-  // damping the tool velocity would need a broadcast too; there every lane integrates
-  // both axes (rows 0 and 1), which measured faster.
+  // Modal state.  Linear cuts split it: the group's lower half integrates the x modes and
+  // its upper half the y modes (row 0 holds this half's axis), which halves the update and
+  // the force sum at the price of a broadcast of x and y on the step's critical path.  With
+  // process damping the tool velocity would need a broadcast too; there every lane
+  // integrates both axes (rows 0 and 1), which measured faster.
   constexpr bool kSplit = !NL;
-  const bool upper = lane >= 16;
+  const bool upper = ll >= (gs >> 1);
   T mk[2][NM], mcd[2][NM], ma[2][NM], q[2][NM], v[2][NM];
 #pragma unroll
   for (int a = 0; a < 2; a++)
@@ -243,9 +320,12 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
   const bool size_effect = NL && P->mc != 0.0;
   const bool pd = NL && pdK != 0.0;
   const int nsteps = P->nsteps, decim = P->decim, ts_c0 = P->ts_c0, h0 = P->hist_h0;
+  const int n_ts = P->ts_n;
   int phc = 0, dcnt = 0, tcount = 0, hcount = 0, eng = 0;
-  float tsx = 0.f, tsy = 0.f, shx = 0.f, shy = 0.f;
-  // FP64 sums of the history window, one per lane: sum dx, sum dy, sum dx^2, sum dy^2
+  float shx = 0.f, shy = 0.f;
+  float tsx = 0.f, tsy = 0.f;  // without groups lane t keeps tooth sample t
+  // FP64 sums of the history window, one per lane of the group's first four: sum dx,
+  // sum dy, sum dx^2, sum dy^2
   double acc = 0.0;
 
   for (int step = 0; step < nsteps; step++) {
@@ -270,8 +350,8 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
         int i = u - cph[s];
         if (i < 0) i += N;
         const T dRi = __shfl_sync(kFull, dRl, i);
-        // idle lanes (no in-cut tooth this round, or a slice past nz whose ring row does not
-        // exist) read a valid table entry and neither read nor write the ring
+        // idle lanes (no in-cut tooth this round, or a slice past nz whose ring row is not
+        // this trial's) read a valid table entry and neither read nor write the ring
         const int j = act[s] ? jj[s] : 0;
         int p = p0[s] + j;  // table position of tooth i at this step (p0 < spr, j < spr)
         if (p >= spr) p -= spr;
@@ -301,8 +381,8 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     }
     // modal integration, semi-implicit Euler; padded modes have k = c = dt/m = 0
     if (kSplit) {
-      // this half's force (Fx in lanes 0-15, Fy in lanes 16-31) drives this half's axis
-      const T F = warp_sum_xy(Fx, Fy, upper);
+      // this half's force (Fx in the lower half, Fy in the upper) drives this half's axis
+      const T F = group_sum_xy(Fx, Fy, upper, gs, lane);
       T qs = T(0);
 #pragma unroll
       for (int j = 0; j < NM; j++) {
@@ -311,11 +391,11 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
         q[0][j] = A::madd(v[0][j], dt, q[0][j]);
         qs += q[0][j];
       }
-      x = __shfl_sync(kFull, qs, 0);
-      y = __shfl_sync(kFull, qs, 16);
+      x = __shfl_sync(kFull, qs, gb);
+      y = __shfl_sync(kFull, qs, gb + (gs >> 1));
     } else {
-      Fx = warp_sum(Fx);
-      Fy = warp_sum(Fy);
+      Fx = group_sum(Fx, gs);
+      Fy = group_sum(Fy, gs);
       T xs = T(0), ys = T(0), vxa = T(0), vya = T(0);
 #pragma unroll
       for (int j = 0; j < NM; j++) {
@@ -345,7 +425,11 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
     }
     if (++phc == spt) {  // once-per-tooth sample (cutting.js:266-268), Float32Array
       phc = 0;
-      if (tcount - ts_c0 == lane) {
+      const int t = tcount - ts_c0;
+      if (GR) {
+        if (ll == 0 && t >= 0 && t < n_ts)
+          samples[gi * kToothSamples + t] = make_float2((float)x, (float)y);
+      } else if (t == lane) {
         tsx = (float)x;
         tsy = (float)y;
       }
@@ -359,42 +443,130 @@ __device__ TrialOut simulate_trial(const PointParams* __restrict__ P, double ap,
           shx = hx;
           shy = hy;
         }
-        const double d = (lane & 1) ? (double)hy - (double)shy : (double)hx - (double)shx;
-        acc = (lane & 2) ? fma(d, d, acc) : acc + d;
+        const double d = (ll & 1) ? (double)hy - (double)shy : (double)hx - (double)shx;
+        acc = (ll & 2) ? fma(d, d, acc) : acc + d;
       }
       hcount++;
     }
   }
 
-  // ---- chatterIndex (cutting.js:299-318) in FP64 ----
-  res.engaged = (unsigned long long)__reduce_add_sync(kFull, (unsigned)eng);
-  res.evals = (unsigned long long)nsteps * (unsigned long long)(N * nz);
-  const double sx = __shfl_sync(kFull, acc, 0), sy = __shfl_sync(kFull, acc, 1),
-               sxx = __shfl_sync(kFull, acc, 2), syy = __shfl_sync(kFull, acc, 3);
-  const int n = P->ts_n;
-  if (n < 8) {
-    res.index = 0.0;
-    res.once = 0.0;
-    res.amp = 0.0;
-  } else {
-    const bool mine = lane < n;
-    const double tx = mine ? (double)tsx : 0.0, ty = mine ? (double)tsy : 0.0;
-    const double mx = warp_sum(tx) / n, my = warp_sum(ty) / n;
-    const double ex = mine ? (double)tsx - mx : 0.0, ey = mine ? (double)tsy - my : 0.0;
-    const double vv = warp_sum(ex * ex + ey * ey);
-    const double once = sqrt(vv / n) * 1e6;
-    const double md = P->hist_m ? (double)P->hist_m : 1.0;
-    double w = (sxx - sx * sx / md) + (syy - sy * sy / md);
-    if (w < 0.0) w = 0.0;  // rounding of the one-pass form; a NaN (run-away cut) stays NaN
-    const double amp = sqrt(w / md);
-    res.once = once;
-    res.amp = amp;
-    res.index = once / (amp + 0.05);
+  // ---- chatterIndex (cutting.js:299-318) in FP64, one group after the other ----
+  const int eng_g = group_sum_int(eng, gs);
+  const bool fin = isfinite((double)x) && isfinite((double)y);
+  __syncwarp();  // the samples are in shared memory
+#pragma unroll 1
+  for (int g = 0; g < (GR ? G.n : 1); g++) {
+    const int b0 = GR ? G.base[g] : 0;
+    TrialOut res;
+    res.engaged = (unsigned long long)__shfl_sync(kFull, eng_g, b0);
+    const int nz_g = __shfl_sync(kFull, nz, b0);
+    res.evals = (unsigned long long)nsteps * (unsigned long long)(N * nz_g);
+    const double sx = __shfl_sync(kFull, acc, b0), sy = __shfl_sync(kFull, acc, b0 + 1),
+                 sxx = __shfl_sync(kFull, acc, b0 + 2), syy = __shfl_sync(kFull, acc, b0 + 3);
+    const int n = n_ts;
+    if (n < 8) {
+      res.index = 0.0;
+      res.once = 0.0;
+      res.amp = 0.0;
+    } else {
+      const bool mine = lane < n;
+      const float2 ts = !mine ? make_float2(0.f, 0.f)
+                        : GR ? samples[g * kToothSamples + lane] : make_float2(tsx, tsy);
+      const double tx = mine ? (double)ts.x : 0.0, ty = mine ? (double)ts.y : 0.0;
+      const double mx = warp_sum(tx) / n, my = warp_sum(ty) / n;
+      const double ex = mine ? (double)ts.x - mx : 0.0, ey = mine ? (double)ts.y - my : 0.0;
+      const double vv = warp_sum(ex * ex + ey * ey);
+      const double once = sqrt(vv / n) * 1e6;
+      const double md = P->hist_m ? (double)P->hist_m : 1.0;
+      double w = (sxx - sx * sx / md) + (syy - sy * sy / md);
+      if (w < 0.0) w = 0.0;  // rounding of the one-pass form; a NaN (run-away cut) stays NaN
+      const double amp = sqrt(w / md);
+      res.once = once;
+      res.amp = amp;
+      res.index = once / (amp + 0.05);
+    }
+    const bool fin_g = __shfl_sync(kFull, fin ? 1 : 0, b0) != 0;
+    res.status = (fin_g && isfinite(res.index)) ? MCS_OK : MCS_ERR_DIVERGED;
+    if (lane == 0) out[g] = res;
   }
-  res.status = (isfinite((double)x) && isfinite((double)y) && isfinite(res.index))
-                   ? MCS_OK
-                   : MCS_ERR_DIVERGED;
-  return res;
+  __syncwarp();
+}
+
+// A single group: the whole warp simulates depth ap.
+__device__ __forceinline__ void one_group(Groups& G, double ap) {
+  G.n = 1;
+  G.base[0] = 0;
+  G.size[0] = kWarp;
+  G.ap[0] = ap;
+#pragma unroll
+  for (int g = 1; g < kMaxGroups; g++) {
+    G.base[g] = kWarp;
+    G.size[g] = 0;
+    G.ap[g] = 0.0;
+  }
+}
+
+// Lane groups for the trials at depths ap[0..n-1] of one point (group g = trial g): a
+// group has the next power of two >= its slice count lanes (at least 4, the history sums
+// need 4), placed first-fit at an aligned offset; the lanes left over form groups without
+// slices.  False when the trials do not fit in one warp.
+__device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, const double* ap,
+                                            int n, Groups& G) {
+  if (n > kMaxGroups) return false;
+  unsigned used = 0u;
+  for (int t = 0; t < n; t++) {
+    int nz;
+    double dz;
+    slice_rule(P, ap[t], nz, dz);
+    int sz = 4;
+    while (sz < nz) sz <<= 1;
+    if (sz > kWarp) return false;
+    const unsigned mask = sz == kWarp ? 0xffffffffu : ((1u << sz) - 1u);
+    int off = -1;
+    for (int o = 0; o < kWarp; o += sz)
+      if ((used & (mask << o)) == 0u) {
+        off = o;
+        break;
+      }
+    if (off < 0) return false;
+    used |= mask << off;
+    G.base[t] = off;
+    G.size[t] = sz;
+    G.ap[t] = ap[t];
+  }
+  int ng = n;
+  for (int sz = 16; sz >= 4; sz >>= 1)  // cover the free lanes with empty groups
+    for (int o = 0; o < kWarp; o += sz) {
+      const unsigned mask = (1u << sz) - 1u;
+      if ((used & (mask << o)) == 0u) {
+        if (ng >= kMaxGroups) return false;
+        used |= mask << o;
+        G.base[ng] = o;
+        G.size[ng] = sz;
+        G.ap[ng] = 0.0;
+        ng++;
+      }
+    }
+  for (int g = ng; g < kMaxGroups; g++) {
+    G.base[g] = kWarp;
+    G.size[g] = 0;
+    G.ap[g] = 0.0;
+  }
+  G.n = ng;
+  return true;
+}
+
+// One trial on the whole warp.
+template <typename T, int SLOTS, int NM, bool NL>
+__device__ __forceinline__ TrialOut simulate_trial(const PointParams* __restrict__ P,
+                                                   double ap,
+                                                   const typename Arith<T>::V2* __restrict__ table,
+                                                   float* __restrict__ ring, float2* samples,
+                                                   TrialOut* out, int lane) {
+  Groups G;
+  one_group(G, ap);
+  simulate<T, SLOTS, NM, NL, false>(P, G, table, ring, samples, out, lane);
+  return out[0];
 }
 
 __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane) {
@@ -404,7 +576,7 @@ __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane
 }
 
 // Persistent solve: each warp takes points from the queue and runs timeDomainLimit.
-template <typename T, int SLOTS, int NM, bool NL>
+template <typename T, int SLOTS, int NM, bool NL, bool GR>
 __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const PointParams* __restrict__ pts,
                                                       const int32_t* __restrict__ order, int n,
                                                       DevOpts o, mcs_result* __restrict__ out,
@@ -422,6 +594,10 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
     const PointParams* P = pts + pi;
     auto* table = reinterpret_cast<typename Arith<T>::V2*>(smem);
     float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr, sizeof(T) == 8));
+    unsigned char* extra =
+        smem + extra_offset(P->spr, sizeof(T) == 8, P->ring_rows, P->lpad);
+    float2* samples = reinterpret_cast<float2*>(extra);
+    TrialOut* outs = reinterpret_cast<TrialOut*>(extra + P->groups * kToothSamples * 8);
     mcs_result r;
     r.status = MCS_OK;
     r.trials = 0;
@@ -434,31 +610,37 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
       r.status = MCS_ERR_CANCELLED;
     } else {
       build_table<T>(P, table, lane);
-      auto chatter = [&](double ap) -> bool {
-        const TrialOut t = simulate_trial<T, SLOTS, NM, NL>(P, ap, table, ring, lane);
+      // a trial on the decision path: its counters join the point's, and its decision
+      auto account = [&](const TrialOut& t) -> bool {
         r.trials++;
         r.evals += t.evals;
         r.engaged += t.engaged;
         if (t.status != MCS_OK) r.status = t.status;
         return t.index > o.chatter_idx;
       };
-      // timeDomainLimit (stabtd.js:24-32) as a state machine around ONE trial call site
-      // (the trial is inlined once): the plain first trial at a_max, then either the
-      // plain geometric bisection over [a_min, a_max] or, with a surrogate guide, the
-      // bracket exp(mu -+ hw) kept inside [a_min, a_max], verified at its upper (chatter)
-      // and lower (stable) end and refined by the same bisection.  A failed verification
-      // falls back to the plain bisection, whose a_max trial has already run.
+      // timeDomainLimit (stabtd.js:24-32) as a state machine of rounds around ONE call of
+      // the trial code (inlined once).  A round is one trial on the whole warp, or several
+      // trials of this point in lane groups: the next bisection levels run speculatively
+      // (the midpoints of a subtree, computed by the same square roots the serial
+      // bisection takes), and only the trials on the decision path are counted, so the
+      // results are those of one trial at a time.  The states: the plain first trial at
+      // a_max, then either the plain geometric bisection over [a_min, a_max] or, with a
+      // surrogate guide, the bracket exp(mu -+ hw) kept inside [a_min, a_max], verified at
+      // its upper (chatter) and lower (stable) end and refined by the same bisection.  A
+      // failed verification falls back to the plain bisection, whose a_max trial has
+      // already run.
       enum : int { kTop, kGuideHi, kGuideLo, kBisect, kDone };
       const bool guided = g.guide != nullptr && g.guide[pi].y >= 0.f;
+      const bool can_group = GR && P->groups > 1;
       int path = guided ? MCS_PATH_GUIDED : MCS_PATH_DIRECT;
       int state = kTop, it = 0, iters = o.iters;
       double lo = o.a_min, hi = o.a_max, glo = 0.0, ghi = 0.0;
       // enter the bisection of [l, h] for n iterations
-      auto bisect = [&](double l, double h, int n) {
+      auto bisect = [&](double l, double h, int nit) {
         lo = l;
         hi = h;
         it = 0;
-        iters = n;
+        iters = nit;
         state = kBisect;
       };
       auto fallback = [&]() {
@@ -468,11 +650,17 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
       // enough halvings that the final bracket is no wider than a hw_min bracket's after
       // `refine` halvings
       auto refine = [&]() {
-        int n = g.refine;
-        for (double w = log(ghi / glo) * 0.5; w > 1.0000001 * (double)g.hw_min; w *= 0.5) n++;
-        bisect(glo, ghi, n);
+        int nit = g.refine;
+        for (double w = log(ghi / glo) * 0.5; w > 1.0000001 * (double)g.hw_min; w *= 0.5) nit++;
+        bisect(glo, ghi, nit);
       };
+      double m[7];
       while (state != kDone) {
+        // ---- plan the round ----
+        Groups G;
+        one_group(G, 0.0);
+        int levels = 0;     // bisection levels the round decides
+        bool both = false;  // both ends of a guide bracket checked in this round
         if (state == kBisect) {
           if (it >= iters) {
             r.alim = sqrt(lo * hi);
@@ -488,67 +676,102 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
             r.hi = hi;
             break;
           }
+          const int lv = min(3, iters - it);
+          m[0] = sqrt(lo * hi);
+          if (lv >= 2) {
+            m[1] = sqrt(lo * m[0]);
+            m[2] = sqrt(m[0] * hi);
+          }
+          if (lv >= 3) {
+            m[3] = sqrt(lo * m[1]);
+            m[4] = sqrt(m[1] * m[0]);
+            m[5] = sqrt(m[0] * m[2]);
+            m[6] = sqrt(m[2] * hi);
+          }
+          levels = 1;
+          if (can_group)
+            for (int d = lv; d >= 2; d--)
+              if (pack_groups(P, m, (1 << d) - 1, G)) {
+                levels = d;
+                break;
+              }
+          if (levels == 1) G.ap[0] = m[0];
+        } else if (state == kTop) {
+          G.ap[0] = o.a_max;
+        } else if (state == kGuideHi) {
+          G.ap[0] = ghi;
+          if (can_group && glo > o.a_min) {
+            const double ends[2] = {ghi, glo};
+            both = pack_groups(P, ends, 2, G);
+          }
+        } else {  // kGuideLo
+          G.ap[0] = glo;
         }
-        const double ap = state == kTop       ? o.a_max
-                          : state == kGuideHi ? ghi
-                          : state == kGuideLo ? glo
-                                              : sqrt(lo * hi);
-        const bool c = chatter(ap);
-        switch (state) {
-          case kTop:
-            if (!c) {
-              r.alim = o.a_max;
-              r.lo = o.a_max;
-              r.hi = INFINITY;
-              r.open = 1;
-              if (guided) path = MCS_PATH_OPEN;
-              state = kDone;
-            } else if (!guided) {
-              bisect(o.a_min, o.a_max, o.iters);
-            } else {
-              const float2 gd = g.guide[pi];
-              const double hw = (double)gd.y;
-              glo = exp((double)gd.x - hw);
-              ghi = exp((double)gd.x + hw);
-              if (glo < o.a_min) {  // shift up to start at a_min
-                glo = o.a_min;
-                ghi = fmin(fmax(ghi, o.a_min * exp(2.0 * hw)), o.a_max);
-              }
-              if (ghi > o.a_max) {  // shift down to end at a_max
-                ghi = o.a_max;
-                glo = fmax(fmin(glo, o.a_max * exp(-2.0 * hw)), o.a_min);
-              }
-              if (!(glo < ghi))
-                fallback();
-              else if (ghi < o.a_max)  // a_max is known to chatter
-                state = kGuideHi;
-              else if (glo > o.a_min)  // a_min is taken as stable, as the plain method does
-                state = kGuideLo;
-              else
-                refine();
+        // ---- run ----
+        simulate<T, SLOTS, NM, NL, GR>(P, G, table, ring, samples, outs, lane);
+        // ---- decide ----
+        if (state == kBisect) {
+          int node = 0;
+          for (int d = 0; d < levels; d++) {
+            const bool c = account(outs[node]);
+            if (c)
+              hi = m[node];
+            else
+              lo = m[node];
+            it++;
+            node = 2 * node + (c ? 1 : 2);
+          }
+        } else if (state == kTop) {
+          const bool c = account(outs[0]);
+          if (!c) {
+            r.alim = o.a_max;
+            r.lo = o.a_max;
+            r.hi = INFINITY;
+            r.open = 1;
+            if (guided) path = MCS_PATH_OPEN;
+            state = kDone;
+          } else if (!guided) {
+            bisect(o.a_min, o.a_max, o.iters);
+          } else {
+            const float2 gd = g.guide[pi];
+            const double hw = (double)gd.y;
+            glo = exp((double)gd.x - hw);
+            ghi = exp((double)gd.x + hw);
+            if (glo < o.a_min) {  // shift up to start at a_min
+              glo = o.a_min;
+              ghi = fmin(fmax(ghi, o.a_min * exp(2.0 * hw)), o.a_max);
             }
-            break;
-          case kGuideHi:
-            if (!c)
+            if (ghi > o.a_max) {  // shift down to end at a_max
+              ghi = o.a_max;
+              glo = fmax(fmin(glo, o.a_max * exp(-2.0 * hw)), o.a_min);
+            }
+            if (!(glo < ghi))
               fallback();
-            else if (glo > o.a_min)
+            else if (ghi < o.a_max)  // a_max is known to chatter
+              state = kGuideHi;
+            else if (glo > o.a_min)  // a_min is taken as stable, as the plain method does
               state = kGuideLo;
             else
               refine();
-            break;
-          case kGuideLo:
-            if (c)
+          }
+        } else if (state == kGuideHi) {
+          if (!account(outs[0]))
+            fallback();
+          else if (glo > o.a_min) {
+            if (!both)
+              state = kGuideLo;
+            else if (account(outs[1]))
               fallback();
             else
               refine();
-            break;
-          default:  // kBisect
-            if (c)
-              hi = ap;
-            else
-              lo = ap;
-            it++;
-            break;
+          } else {
+            refine();
+          }
+        } else {  // kGuideLo
+          if (account(outs[0]))
+            fallback();
+          else
+            refine();
         }
       }
       if (g.info != nullptr && lane == 0) {
@@ -586,8 +809,14 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) trials_kernel(const
     const PointParams* P = pts + it.point;
     auto* table = reinterpret_cast<typename Arith<T>::V2*>(smem);
     float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr, sizeof(T) == 8));
+    int nz;
+    double dz;
+    slice_rule(P, it.ap, nz, dz);  // this item's shared memory holds nz ring rows
+    unsigned char* extra = smem + extra_offset(P->spr, sizeof(T) == 8, nz, P->lpad);
+    float2* samples = reinterpret_cast<float2*>(extra);
+    TrialOut* outs = reinterpret_cast<TrialOut*>(extra + kToothSamples * 8);
     build_table<T>(P, table, lane);
-    const TrialOut t = simulate_trial<T, SLOTS, NM, NL>(P, it.ap, table, ring, lane);
+    const TrialOut t = simulate_trial<T, SLOTS, NM, NL>(P, it.ap, table, ring, samples, outs, lane);
     if (lane == 0) {
       mcs_trial_result r;
       r.index = t.index;
@@ -602,9 +831,12 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) trials_kernel(const
 }
 
 template <typename T, int SLOTS, int NM>
-void* solve_fn(bool nl) {
-  return nl ? reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, true>)
-            : reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, false>);
+void* solve_fn(bool nl, bool gr) {
+  if (gr)
+    return nl ? reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, true, true>)
+              : reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, false, true>);
+  return nl ? reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, true, false>)
+            : reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, false, false>);
 }
 template <typename T, int SLOTS, int NM>
 void* trials_fn(bool nl) {
@@ -615,8 +847,10 @@ void* trials_fn(bool nl) {
 void* pick(bool solve, const KernelShape& s) {
 #define MCS_PICK(SL, NMV)                                                              \
   if (s.slots == SL && s.modes == NMV)                                                 \
-    return s.fp64 ? (solve ? solve_fn<double, SL, NMV>(s.nl) : trials_fn<double, SL, NMV>(s.nl)) \
-                  : (solve ? solve_fn<float, SL, NMV>(s.nl) : trials_fn<float, SL, NMV>(s.nl));
+    return s.fp64 ? (solve ? solve_fn<double, SL, NMV>(s.nl, s.grouped)                 \
+                           : trials_fn<double, SL, NMV>(s.nl))                            \
+                  : (solve ? solve_fn<float, SL, NMV>(s.nl, s.grouped)                   \
+                           : trials_fn<float, SL, NMV>(s.nl));
   MCS_PICK(1, 1)
   MCS_PICK(1, 2)
   MCS_PICK(1, 3)
@@ -636,8 +870,8 @@ int set_smem_limits() {
   for (int nl = 0; nl < 2; nl++)
   for (int sl = 1; sl <= kMaxSlots; sl++)
     for (int nm = 1; nm <= kMaxModes; nm++)
-      for (int k = 0; k < 2; k++) {
-        void* f = pick(k == 0, KernelShape{sl, nm, fp, nl});
+      for (int k = 0; k < 3; k++) {  // solve, grouped solve, trials
+        void* f = pick(k < 2, KernelShape{sl, nm, fp, nl, k == 1 ? 1 : 0});
         cudaError_t e =
             cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerWarp);
         if (e != cudaSuccess) return (int)e;

@@ -83,7 +83,7 @@ class Opts(C.Structure):
                 ("revs", C.c_int32), ("nonlinear", C.c_int32), ("honor_runout", C.c_int32),
                 ("steps_per_tooth", C.c_int32), ("slices", C.c_int32),
                 ("chatter_idx", C.c_double), ("precision", C.c_int32),
-                ("max_buckets", C.c_int32)]
+                ("max_buckets", C.c_int32), ("serial_trials", C.c_int32), ("pad", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -178,8 +178,9 @@ def make_setup(tool, mat, arc: Sequence[float], fz: float) -> Setup:
 def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
     """timeDomainLimit/chatterAt options (src/stabtd.js:14,24) with the reference defaults,
     plus the explicit extensions honorRunout, stepsPerTooth, slices, chatterIdx,
-    precision ("fp32": FP32 force law and modal integration, "fp64": FP64) and maxBuckets
-    (the schedule; 0 = the library's default, see mcs.tune)."""
+    precision ("fp32": FP32 force law and modal integration, "fp64": FP64), maxBuckets
+    (the schedule; 0 = the library's default, see mcs.tune) and serialTrials (True: one
+    bisection trial at a time instead of speculative lane groups; same results)."""
     d = dict(DEFAULTS)
     if o:
         d.update(o)
@@ -189,7 +190,7 @@ def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
                 1 if d.get("honorRunout", False) else 0,
                 int(d.get("stepsPerTooth", 0) or 0), int(d.get("slices", 0) or 0),
                 float(d.get("chatterIdx", CHATTER_IDX)), precision_code(d.get("precision")),
-                int(d.get("maxBuckets", 0) or 0))
+                int(d.get("maxBuckets", 0) or 0), 1 if d.get("serialTrials", False) else 0, 0)
 
 
 FP32 = 0
@@ -257,7 +258,8 @@ TRIAL_DTYPE = np.dtype([("point", "<u4"), ("pad", "<u4"), ("ap", "<f8")])
 OPTS_DTYPE = np.dtype([("a_min", "<f8"), ("a_max", "<f8"), ("iters", "<i4"), ("revs", "<i4"),
                        ("nonlinear", "<i4"), ("honor_runout", "<i4"),
                        ("steps_per_tooth", "<i4"), ("slices", "<i4"), ("chatter_idx", "<f8"),
-                       ("precision", "<i4"), ("max_buckets", "<i4")])
+                       ("precision", "<i4"), ("max_buckets", "<i4"),
+                       ("serial_trials", "<i4"), ("pad", "<i4")])
 for _d, _c in ((MODAL_DTYPE, Modal), (SETUP_DTYPE, Setup), (POINT_DTYPE, Point),
                (TRIAL_DTYPE, Trial), (OPTS_DTYPE, Opts)):
     assert _d.itemsize == C.sizeof(_c), (_d, _c)
@@ -280,6 +282,13 @@ def as_records(items, dtype) -> np.ndarray:
 
 def opts_record(o: Opts) -> np.ndarray:
     return np.frombuffer(bytes(o), dtype=OPTS_DTYPE).copy()
+
+
+def opts_from_record(rec) -> Opts:
+    """Opts from a stored record; records written before fields were added end early and
+    the missing trailing fields read as 0 (their defaults)."""
+    raw = np.asarray(rec).tobytes()
+    return Opts.from_buffer_copy(raw + bytes(max(0, C.sizeof(Opts) - len(raw))))
 
 
 # ---------------------------------------------------------------- surrogate

@@ -15,7 +15,7 @@ def oracle_run(oracle, g, idx):
     modals = [A.Modal.from_buffer_copy(r.tobytes()) for r in g["modals"]]
     pts = g["points"][idx]
     P = (A.Point * len(pts)).from_buffer_copy(pts.tobytes())
-    opts = A.Opts.from_buffer_copy(g["opts"].tobytes())
+    opts = A.opts_from_record(g["opts"])
     return oracle.solve_batch(setups, modals, P, opts, nthreads=0, traces=True)
 
 

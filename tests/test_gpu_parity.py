@@ -43,7 +43,7 @@ PRECISIONS = ["fp32", "fp64"]
 def opts_of(g, precision="fp32"):
     from mcs import _abi as A
 
-    o = A.Opts.from_buffer_copy(g["opts"].tobytes())
+    o = A.opts_from_record(g["opts"])
     o.precision = A.precision_code(precision)
     return o
 

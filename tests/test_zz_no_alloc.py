@@ -40,7 +40,7 @@ def _solve(ctx, fn_name, g, opts):
 def _opts(g, **kw):
     from mcs import _abi as A
 
-    o = A.Opts.from_buffer_copy(g["opts"].tobytes())
+    o = A.opts_from_record(g["opts"])
     for k, v in kw.items():
         setattr(o, k, v)
     return o
