@@ -37,6 +37,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "machinig-sim_b200"))
 sys.path.insert(0, str(ROOT / "oracle"))
 
+WORKLOADS = {
+    "sweep": "sweep: 4096 speeds 3000-30000 rpm, 4-flute D10 helix 30, 3+3 modes, 10 um "
+             "runout, [0.05,15] x 10, 60 revs, 40 slices",
+    "hetero": "hetero: 16384 seeded setups (D 3-20 mm, 2-6 flutes, helix 0-45, runout 0-20 um, "
+              "1-3 modes per axis, process damping and size effect), [0.05,15] x 10, 60 revs, "
+              "reference slice rule",
+}
 METRIC = "stability-boundary points/sec on 1 B200: surrogate-guided vs plain GPU vs Node CPU @<=2% depth err"
 UNIT = "points/s"
 FLOP_ENGAGED = 46.0   # FP32 flop per in-cut slice evaluation (force law, cutting.js:181-207)
@@ -144,7 +151,7 @@ def cpu_baseline(wl, target_s: float = 15.0) -> dict:
         if n2 > npts:
             npts, dt = run_oracle_sample(wl, n2, cores)
     return {"value": npts / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{npts} of the {wl.n} sweep points (seeded), C++ FP64 restatement of "
+            "sample": f"{npts} of the {wl.n} {wl.name} points (seeded), C++ FP64 restatement of "
                       f"stabtd.js/cutting.js, {cores} threads on {cpu_model()}"}
 
 
@@ -245,7 +252,7 @@ def reference_arm(args) -> int:
         return 0
     from mcs import workloads as W
 
-    wl = W.sweep()
+    wl = W.hetero(n=16384) if args.workload == "hetero" else W.sweep()
     cores = cpu_cores()
     n = min(wl.n, max(8, cores))
     for _ in range(args.warmup):
@@ -261,11 +268,10 @@ def reference_arm(args) -> int:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {"workload": "sweep: 4096 speeds 3000-30000 rpm, 4-flute D10, 3+3 modes, "
-                               "10 um runout, [0.05,15] x 10, 60 revs, 40 slices",
+        "config": {"workload": WORKLOADS[args.workload],
                    "sample_points_per_step": n},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{n} seeded sweep points per step; the reference is "
+                         "sample": f"{n} seeded {wl.name} points per step; the reference is "
                                    f"JavaScript with no JS runtime on this box, so its C++ "
                                    f"FP64 restatement runs, {cores} threads, {cpu_model()}"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -291,9 +297,14 @@ def ours(args) -> int:
     from mcs import tune as T
     from mcs import workloads as W
 
-    wl = W.sweep(seed=1 + rank)
-    if args.points and args.points < wl.n:  # a smaller case of the same sweep (profiling)
+    if args.workload == "hetero":  # 16384 seeded setups per rank (weak scaling)
+        wl = W.hetero(n=16384, first_seed=16384 * rank)
+    else:
+        wl = W.sweep(seed=1 + rank)
+    if args.points and args.points < wl.n:  # a smaller case of the same workload (profiling)
         wl = wl.subset(np.linspace(0, wl.n - 1, args.points).round().astype(int))
+    if args.serial_trials:
+        wl.opts.serial_trials = 1
     ctx = mcs.Context(device)
     stream = torch.cuda.ExternalStream(ctx.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
@@ -313,11 +324,14 @@ def ours(args) -> int:
         """Device-resident plan of the sweep: per-step CUDA-event times, results, info."""
         opts = A.make_opts(precision=precision)
         for f in ("a_min", "a_max", "iters", "revs", "nonlinear", "honor_runout",
-                  "steps_per_tooth", "slices", "chatter_idx"):
+                  "steps_per_tooth", "slices", "chatter_idx", "serial_trials"):
             setattr(opts, f, getattr(wl.opts, f))
         # schedule (number of shared-memory size classes) from the autotuner, untimed
-        opts.max_buckets, tuned = T.autotune(ctx, wl.setups, wl.modals, wl.points, opts,
-                                             device_name=torch.cuda.get_device_name(device))
+        if args.max_buckets:
+            opts.max_buckets, tuned = args.max_buckets, {"ms": {}, "cached": False}
+        else:
+            opts.max_buckets, tuned = T.autotune(ctx, wl.setups, wl.modals, wl.points, opts,
+                                                 device_name=torch.cuda.get_device_name(device))
         plan = ctx.plan(wl.setups, wl.modals, wl.points, opts)
         info = plan.info()
         info["schedule"] = {"max_buckets": int(opts.max_buckets), "tuning_ms": tuned["ms"],
@@ -417,8 +431,7 @@ def ours(args) -> int:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32" else "f64",
             "data": "synthetic (seeded sweep; no public dataset exists for this path)",
-            "config": {"workload": "sweep: 4096 speeds 3000-30000 rpm, 4-flute D10 helix 30, "
-                                   "3+3 modes, 10 um runout, [0.05,15] x 10, 60 revs, 40 slices",
+            "config": {"workload": WORKLOADS[args.workload],
                        "points_per_gpu": wl.n,
                        "variant": f"plain GPU bisection, {args.precision} force law and "
                                   "modal integration, FP64 statistics and bracket",
@@ -464,10 +477,16 @@ def main(argv=None) -> int:
                     help="integration precision of the headline value")
     ap.add_argument("--fp32-only", action="store_true", help="time only the headline precision")
     ap.add_argument("--points", type=int, default=0,
-                    help="solve an evenly spaced subset of the sweep (profiling case)")
+                    help="solve an evenly spaced subset of the workload (profiling case)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-guided", action="store_true",
                     help="skip the surrogate-guided serving leg")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "hetero"],
+                    help="sweep (the headline) or the heterogeneous batch")
+    ap.add_argument("--max-buckets", type=int, default=0,
+                    help="fixed schedule (shared-memory size classes); 0: autotune")
+    ap.add_argument("--serial-trials", action="store_true",
+                    help="one bisection trial per warp at a time (same results)")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         a.warmup = 3

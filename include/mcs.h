@@ -268,7 +268,8 @@ int mcs_solve_noalloc(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,
  * the batch for every candidate max_buckets (at most 64 candidates), runs each once
  * untimed, then times three round-robin rounds of one execution per candidate, each after
  * a write of twice the L2 size (so from a cold L2; the tuner allocates that buffer).  ms[]
- * (NULL allowed) receives each candidate's fastest round and *best the fastest candidate.
+ * (NULL allowed) receives each candidate's mean over the rounds and *best the fastest
+ * candidate by that mean.
  * opts->max_buckets is ignored.  Results of a solve are identical for every schedule; only
  * the time changes.
  */

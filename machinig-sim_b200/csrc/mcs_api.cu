@@ -827,10 +827,11 @@ int mcs_tune(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_mod
   MCS_CUDA(cudaSetDevice(c->device));
   // all candidate plans first; then kRounds rounds in which every candidate runs once,
   // round-robin, so that a drift of the clocks does not favour one candidate; each
-  // candidate's time is its fastest round
+  // candidate's time is its mean over the rounds: schedules with many concurrent grids
+  // vary from run to run (their start order races), and a best-of ranking chose them
   constexpr int kRounds = 3;
   std::vector<mcs_plan*> plans(n_candidates, nullptr);
-  std::vector<double> t(n_candidates, INFINITY);
+  std::vector<double> t(n_candidates, 0.0);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int rc = MCS_OK;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
@@ -869,7 +870,7 @@ int mcs_tune(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_mod
       if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
       if (e == cudaSuccess) e = cudaEventSynchronize(e1);
       if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
-      if (e == cudaSuccess) t[i] = std::min(t[i], (double)f);
+      if (e == cudaSuccess) t[i] += (double)f / kRounds;
     }
   }
   cudaStreamSynchronize(c->stream);
