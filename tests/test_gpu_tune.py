@@ -62,3 +62,31 @@ def test_autotune_caches_its_choice(ctx, tmp_path):
     best2, rec2 = T.autotune(ctx, wl.setups, wl.modals, wl.points, wl.opts,
                              candidates=(4, 16), cache=path)
     assert rec2["cached"] and best2 == best
+
+
+def test_lane_group_trials_match_serial_trials(ctx):
+    """Speculative bisection levels run in lane groups give byte-identical results to one
+    trial at a time (plain solve, plan and guided solve; the same counters too)."""
+    from mcs import _abi as A
+    from mcs import surrogate as SG
+    from mcs import workloads as W
+
+    wl = W.hetero(n=1024, first_seed=31337)
+    serial = A.Opts.from_buffer_copy(bytes(wl.opts))
+    serial.serial_trials = 1
+    a = ctx.solve(wl.setups, wl.modals, wl.points, serial)
+    b = ctx.solve(wl.setups, wl.modals, wl.points, wl.opts)
+    assert a.tobytes() == b.tobytes()
+    plan = ctx.plan(wl.setups, wl.modals, wl.points, wl.opts)
+    plan.execute()
+    assert plan.results().tobytes() == a.tobytes()
+    plan.close()
+    s = SG.load(ctx)
+    ga, ia = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, serial)
+    gb, ib = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts)
+    assert ga.tobytes() == gb.tobytes() and ia.tobytes() == ib.tobytes()
+    s.close()
+    with pytest.raises(Exception):
+        bad = A.Opts.from_buffer_copy(bytes(wl.opts))
+        bad.serial_trials = 2
+        ctx.solve(wl.setups, wl.modals, wl.points, bad)

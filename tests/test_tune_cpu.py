@@ -51,3 +51,17 @@ def test_opts_carry_the_schedule():
     assert A.make_opts().max_buckets == 0
     assert A.make_opts(maxBuckets=12).max_buckets == 12
     assert A.OPTS_DTYPE.itemsize == __import__("ctypes").sizeof(A.Opts)
+
+
+def test_old_option_records_read_with_defaults():
+    """Option records stored before the schedule fields existed read them as 0."""
+    import ctypes as C
+
+    from mcs import _abi as A
+
+    o = A.make_opts(maxBuckets=0)
+    old = np.frombuffer(bytes(o), dtype=np.uint8)[:56].copy()  # the 56-byte layout
+    r = A.opts_from_record(old)
+    assert r.max_buckets == 0 and r.serial_trials == 0 and r.a_max == o.a_max
+    assert C.sizeof(A.Opts) == 64
+    assert A.make_opts(serialTrials=True).serial_trials == 1
