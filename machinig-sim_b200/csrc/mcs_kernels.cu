@@ -7,14 +7,18 @@
 // Work layout inside a warp (the run() loop of src/cutting.js:168-293):
 //   * lane l owns axial slices l and l + 32 (SLOTS = 1 or 2 -> nz <= 64); the slice
 //     geometry (cutting.js:98-124) lives in registers for the whole trial;
-//   * per step the N teeth are visited in turn; a tooth whose slices are all outside
-//     the engaged arc is skipped by the whole warp (vote), otherwise every lane whose
-//     slice is in cut evaluates the force law (cutting.js:181-207) in FP32 (or FP64
-//     when the caller asks for it: the kernels are templated on the scalar type);
-//   * Fx, Fy are summed with a butterfly of shuffles, so every lane holds the total and
-//     runs the modal update (semi-implicit Euler, cutting.js:246-255) redundantly;
+//   * each lane follows its slices' own phase in the revolution and visits only the teeth
+//     in cut there (predicated rounds over both slots); every in-cut lane evaluates the
+//     force law (cutting.js:181-207) in FP32 (or FP64 when the caller asks for it: the
+//     kernels are templated on the scalar type);
+//   * Fx, Fy are summed with a butterfly of shuffles.  Linear cuts split the modal update
+//     (semi-implicit Euler, cutting.js:246-255) between the half-warps, one axis each;
+//     with process damping every lane integrates both axes;
 //   * the once-per-tooth samples of the chatter-index window sit one per lane, and the
 //     decimated-history statistics are accumulated in FP64 (cutting.js:265-292,299-318).
+// A trial whose slices fit a smaller aligned group of lanes can share the warp with other
+// trials of the same point: the bisection runs its next levels speculatively in lane
+// groups, each of which computes exactly what a whole warp would (simulate, Groups).
 //
 // The delayed surface: the reference keeps surf[slice][position] for a whole revolution
 // (cutting.js:62-68).  With the static arc map of chatterAt a (slice, position) cell has
@@ -39,28 +43,9 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr float kLog2HRef = -4.321928094887363f;  // log2(H_REF = 0.05 mm), cutting.js:18
 constexpr float kHMin = 0.002f;                    // cutting.js:19
 
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-
-// Fx summed over the warp into lanes 0-15 and Fy into lanes 16-31, in one butterfly: the
-// xor-16 step adds each lane's partner's share of the other half's force, the next four
-// steps reduce within each half.  Every addition has the same operands as in two separate
-// butterflies, so the sums are bit for bit those of warp_sum(Fx) and warp_sum(Fy).
-template <typename T>
-__device__ __forceinline__ T warp_sum_xy(T fx, T fy, bool upper) {
-  T v = upper ? fy : fx;
-  v += __shfl_xor_sync(kFull, upper ? fx : fy, 16);
-#pragma unroll
-  for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
   return v;
 }
 
