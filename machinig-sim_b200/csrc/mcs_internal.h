@@ -77,7 +77,7 @@ __host__ __device__ inline int table_bytes(int spr, bool fp64) {
 // After the table and the ring: per trial group, its once-per-tooth samples (float2) and
 // its result record.  A warp runs up to kMaxGroups trials of one point together in lane
 // groups (speculative bisection levels).
-constexpr int kMaxGroups = 8;
+constexpr int kMaxGroups = 16;
 constexpr int kToothSamples = 24;
 constexpr int kTrialOutBytes = 48;
 __host__ __device__ inline int extra_offset(int spr, bool fp64, int ring_rows, int lpad) {

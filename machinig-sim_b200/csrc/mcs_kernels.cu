@@ -309,9 +309,11 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
   int phc = 0, dcnt = 0, tcount = 0, hcount = 0, eng = 0;
   float shx = 0.f, shy = 0.f;
   float tsx = 0.f, tsy = 0.f;  // without groups lane t keeps tooth sample t
-  // FP64 sums of the history window, one per lane of the group's first four: sum dx,
-  // sum dy, sum dx^2, sum dy^2
-  double acc = 0.0;
+  // FP64 sums of the history window.  Without groups one per lane of lanes 0-3: sum dx,
+  // sum dy, sum dx^2, sum dy^2.  In lane groups (as small as 2 lanes) two per lane of the
+  // group's first two: sum d and sum d^2 of x (lane 0) and of y (lane 1), the same
+  // additions in the same order.
+  double acc = 0.0, acc2 = 0.0;
 
   for (int step = 0; step < nsteps; step++) {
     const T xm = x * T(1e3), ym = y * T(1e3);  // tool position [mm]
@@ -429,7 +431,12 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
           shy = hy;
         }
         const double d = (ll & 1) ? (double)hy - (double)shy : (double)hx - (double)shx;
-        acc = (ll & 2) ? fma(d, d, acc) : acc + d;
+        if (GR) {
+          acc = acc + d;
+          acc2 = fma(d, d, acc2);
+        } else {
+          acc = (ll & 2) ? fma(d, d, acc) : acc + d;
+        }
       }
       hcount++;
     }
@@ -446,8 +453,9 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
     res.engaged = (unsigned long long)__shfl_sync(kFull, eng_g, b0);
     const int nz_g = __shfl_sync(kFull, nz, b0);
     res.evals = (unsigned long long)nsteps * (unsigned long long)(N * nz_g);
-    const double sx = __shfl_sync(kFull, acc, b0), sy = __shfl_sync(kFull, acc, b0 + 1),
-                 sxx = __shfl_sync(kFull, acc, b0 + 2), syy = __shfl_sync(kFull, acc, b0 + 3);
+    const double sx = __shfl_sync(kFull, acc, b0), sy = __shfl_sync(kFull, acc, b0 + 1);
+    const double sxx = __shfl_sync(kFull, GR ? acc2 : acc, GR ? b0 : b0 + 2),
+                 syy = __shfl_sync(kFull, GR ? acc2 : acc, GR ? b0 + 1 : b0 + 3);
     const int n = n_ts;
     if (n < 8) {
       res.index = 0.0;
@@ -492,9 +500,9 @@ __device__ __forceinline__ void one_group(Groups& G, double ap) {
 }
 
 // Lane groups for the trials at depths ap[0..n-1] of one point (group g = trial g): a
-// group has the next power of two >= its slice count lanes (at least 4, the history sums
-// need 4), placed first-fit at an aligned offset; the lanes left over form groups without
-// slices.  False when the trials do not fit in one warp.
+// group has the next power of two >= its slice count lanes (at least 2: the split modal
+// update and the history sums need two), placed first-fit at an aligned offset; the lanes
+// left over form groups without slices.  False when the trials do not fit in one warp.
 __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, const double* ap,
                                             int n, Groups& G) {
   if (n > kMaxGroups) return false;
@@ -503,7 +511,7 @@ __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, c
     int nz;
     double dz;
     slice_rule(P, ap[t], nz, dz);
-    int sz = 4;
+    int sz = 2;
     while (sz < nz) sz <<= 1;
     if (sz > kWarp) return false;
     const unsigned mask = sz == kWarp ? 0xffffffffu : ((1u << sz) - 1u);
@@ -520,7 +528,7 @@ __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, c
     G.ap[t] = ap[t];
   }
   int ng = n;
-  for (int sz = 16; sz >= 4; sz >>= 1)  // cover the free lanes with empty groups
+  for (int sz = 16; sz >= 2; sz >>= 1)  // cover the free lanes with empty groups
     for (int o = 0; o < kWarp; o += sz) {
       const unsigned mask = (1u << sz) - 1u;
       if ((used & (mask << o)) == 0u) {
@@ -639,7 +647,6 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         for (double w = log(ghi / glo) * 0.5; w > 1.0000001 * (double)g.hw_min; w *= 0.5) nit++;
         bisect(glo, ghi, nit);
       };
-      double m[7];
       while (state != kDone) {
         // ---- plan the round ----
         Groups G;
@@ -661,26 +668,31 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
             r.hi = hi;
             break;
           }
-          const int lv = min(3, iters - it);
-          m[0] = sqrt(lo * hi);
-          if (lv >= 2) {
-            m[1] = sqrt(lo * m[0]);
-            m[2] = sqrt(m[0] * hi);
-          }
-          if (lv >= 3) {
-            m[3] = sqrt(lo * m[1]);
-            m[4] = sqrt(m[1] * m[0]);
-            m[5] = sqrt(m[0] * m[2]);
-            m[6] = sqrt(m[2] * hi);
-          }
+          const int lv = min(4, iters - it);
           levels = 1;
-          if (can_group)
+          if (can_group && lv >= 2) {
+            // the speculative subtree: node k brackets [L_k, H_k] with midpoint m_k; its
+            // left child (chatter at m_k) brackets [L_k, m_k], its right child [m_k, H_k]
+            constexpr int kTree = 15;  // 4 levels
+            double m[kTree], L[kTree], H[kTree];
+            L[0] = lo;
+            H[0] = hi;
+            m[0] = sqrt(lo * hi);
+            for (int k = 0; 2 * k + 2 < (1 << lv) - 1; k++) {
+              L[2 * k + 1] = L[k];
+              H[2 * k + 1] = m[k];
+              m[2 * k + 1] = sqrt(L[k] * m[k]);
+              L[2 * k + 2] = m[k];
+              H[2 * k + 2] = H[k];
+              m[2 * k + 2] = sqrt(m[k] * H[k]);
+            }
             for (int d = lv; d >= 2; d--)
               if (pack_groups(P, m, (1 << d) - 1, G)) {
                 levels = d;
                 break;
               }
-          if (levels == 1) G.ap[0] = m[0];
+          }
+          if (levels == 1) G.ap[0] = sqrt(lo * hi);
         } else if (state == kTop) {
           G.ap[0] = o.a_max;
         } else if (state == kGuideHi) {
@@ -696,13 +708,15 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         simulate<T, SLOTS, NM, NL, GR>(P, G, table, ring, samples, outs, lane);
         // ---- decide ----
         if (state == kBisect) {
+          // walk the decision path: node k's midpoint is the serial bisection's sqrt(lo*hi)
           int node = 0;
           for (int d = 0; d < levels; d++) {
+            const double mid = sqrt(lo * hi);
             const bool c = account(outs[node]);
             if (c)
-              hi = m[node];
+              hi = mid;
             else
-              lo = m[node];
+              lo = mid;
             it++;
             node = 2 * node + (c ? 1 : 2);
           }
