@@ -90,3 +90,20 @@ def test_lane_group_trials_match_serial_trials(ctx):
         bad = A.Opts.from_buffer_copy(bytes(wl.opts))
         bad.serial_trials = 2
         ctx.solve(wl.setups, wl.modals, wl.points, bad)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_lane_groups_with_fixed_slice_count(ctx, precision):
+    """A fixed slice count of 16 or fewer also packs trials into lane groups; the results
+    equal one trial at a time in both precisions."""
+    from mcs import _abi as A
+    from mcs import workloads as W
+
+    wl = W.hetero(n=256, first_seed=2024)
+    o = A.make_opts(dict(W.HETERO_OPTS), slices=8, revs=20, precision=precision)
+    s = A.Opts.from_buffer_copy(bytes(o))
+    s.serial_trials = 1
+    a = ctx.solve(wl.setups, wl.modals, wl.points, s)
+    b = ctx.solve(wl.setups, wl.modals, wl.points, o)
+    assert a.tobytes() == b.tobytes()
+    assert np.all(a["trials"] >= 1)
