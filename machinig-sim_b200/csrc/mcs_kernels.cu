@@ -499,13 +499,20 @@ __device__ __forceinline__ void one_group(Groups& G, double ap) {
   }
 }
 
+// A failed packing leaves the single whole-warp group (depth 0; the caller sets it).
+__device__ __forceinline__ bool unpacked(Groups& G) {
+  one_group(G, 0.0);
+  return false;
+}
+
 // Lane groups for the trials at depths ap[0..n-1] of one point (group g = trial g): a
 // group has the next power of two >= its slice count lanes (at least 2: the split modal
 // update and the history sums need two), placed first-fit at an aligned offset; the lanes
-// left over form groups without slices.  False when the trials do not fit in one warp.
+// left over form groups without slices.  False, with G reset to the single whole-warp
+// group, when the trials do not fit in one warp.
 __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, const double* ap,
                                             int n, Groups& G) {
-  if (n > kMaxGroups) return false;
+  if (n > kMaxGroups) return unpacked(G);
   unsigned used = 0u;
   for (int t = 0; t < n; t++) {
     int nz;
@@ -513,7 +520,7 @@ __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, c
     slice_rule(P, ap[t], nz, dz);
     int sz = 2;
     while (sz < nz) sz <<= 1;
-    if (sz > kWarp) return false;
+    if (sz > kWarp) return unpacked(G);
     const unsigned mask = sz == kWarp ? 0xffffffffu : ((1u << sz) - 1u);
     int off = -1;
     for (int o = 0; o < kWarp; o += sz)
@@ -521,7 +528,7 @@ __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, c
         off = o;
         break;
       }
-    if (off < 0) return false;
+    if (off < 0) return unpacked(G);
     used |= mask << off;
     G.base[t] = off;
     G.size[t] = sz;
@@ -532,7 +539,7 @@ __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, c
     for (int o = 0; o < kWarp; o += sz) {
       const unsigned mask = (1u << sz) - 1u;
       if ((used & (mask << o)) == 0u) {
-        if (ng >= kMaxGroups) return false;
+        if (ng >= kMaxGroups) return unpacked(G);
         used |= mask << o;
         G.base[ng] = o;
         G.size[ng] = sz;
@@ -547,6 +554,25 @@ __device__ __forceinline__ bool pack_groups(const PointParams* __restrict__ P, c
   }
   G.n = ng;
   return true;
+}
+
+// The midpoints of the first d levels of a bisection of [lo, hi] in breadth-first order:
+// node k brackets [L_k, H_k] and has midpoint m_k = sqrt(L_k * H_k); its left child (chatter
+// at m_k) brackets [L_k, m_k], its right child [m_k, H_k] -- the square roots the serial
+// bisection takes on every path.
+__device__ __forceinline__ void tree_midpoints(double lo, double hi, int d, double* m) {
+  double L[15], H[15];
+  L[0] = lo;
+  H[0] = hi;
+  m[0] = sqrt(lo * hi);
+  for (int k = 0; 2 * k + 2 < (1 << d) - 1; k++) {
+    L[2 * k + 1] = L[k];
+    H[2 * k + 1] = m[k];
+    m[2 * k + 1] = sqrt(L[k] * m[k]);
+    L[2 * k + 2] = m[k];
+    H[2 * k + 2] = H[k];
+    m[2 * k + 2] = sqrt(m[k] * H[k]);
+  }
 }
 
 // One trial on the whole warp.
@@ -642,17 +668,19 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
       };
       // enough halvings that the final bracket is no wider than a hw_min bracket's after
       // `refine` halvings
-      auto refine = [&]() {
+      auto refine_iters = [&]() {
         int nit = g.refine;
         for (double w = log(ghi / glo) * 0.5; w > 1.0000001 * (double)g.hw_min; w *= 0.5) nit++;
-        bisect(glo, ghi, nit);
+        return nit;
       };
+      auto refine = [&]() { bisect(glo, ghi, refine_iters()); };
       while (state != kDone) {
         // ---- plan the round ----
         Groups G;
         one_group(G, 0.0);
-        int levels = 0;     // bisection levels the round decides
-        bool both = false;  // both ends of a guide bracket checked in this round
+        int levels = 0;       // bisection levels the round decides
+        bool packed = false;  // guide check: the lower end (and spec refinement levels) too
+        int spec = 0;
         if (state == kBisect) {
           if (it >= iters) {
             r.alim = sqrt(lo * hi);
@@ -671,21 +699,8 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
           const int lv = min(4, iters - it);
           levels = 1;
           if (can_group && lv >= 2) {
-            // the speculative subtree: node k brackets [L_k, H_k] with midpoint m_k; its
-            // left child (chatter at m_k) brackets [L_k, m_k], its right child [m_k, H_k]
-            constexpr int kTree = 15;  // 4 levels
-            double m[kTree], L[kTree], H[kTree];
-            L[0] = lo;
-            H[0] = hi;
-            m[0] = sqrt(lo * hi);
-            for (int k = 0; 2 * k + 2 < (1 << lv) - 1; k++) {
-              L[2 * k + 1] = L[k];
-              H[2 * k + 1] = m[k];
-              m[2 * k + 1] = sqrt(L[k] * m[k]);
-              L[2 * k + 2] = m[k];
-              H[2 * k + 2] = H[k];
-              m[2 * k + 2] = sqrt(m[k] * H[k]);
-            }
+            double m[15];  // the speculative subtree, 4 levels at most
+            tree_midpoints(lo, hi, lv, m);
             for (int d = lv; d >= 2; d--)
               if (pack_groups(P, m, (1 << d) - 1, G)) {
                 levels = d;
@@ -696,11 +711,23 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         } else if (state == kTop) {
           G.ap[0] = o.a_max;
         } else if (state == kGuideHi) {
-          G.ap[0] = ghi;
-          if (can_group && glo > o.a_min) {
-            const double ends[2] = {ghi, glo};
-            both = pack_groups(P, ends, 2, G);
+          // the checks of both ends and, speculatively, the first levels of the refinement
+          // that follows when both pass, in one round
+          if (can_group) {
+            double aps[2 + 7];
+            int k0 = 0;
+            aps[k0++] = ghi;
+            if (glo > o.a_min) aps[k0++] = glo;
+            for (int d = min(3, refine_iters()); d >= 0 && !packed; d--) {
+              if (d > 0) tree_midpoints(glo, ghi, d, aps + k0);
+              const int nt = k0 + (1 << d) - 1;
+              if (nt > 1 && pack_groups(P, aps, nt, G)) {
+                packed = true;
+                spec = d;
+              }
+            }
           }
+          if (!packed) G.ap[0] = ghi;
         } else {  // kGuideLo
           G.ap[0] = glo;
         }
@@ -754,17 +781,28 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
               refine();
           }
         } else if (state == kGuideHi) {
-          if (!account(outs[0]))
+          const bool lo_chk = glo > o.a_min;
+          if (!account(outs[0])) {
             fallback();
-          else if (glo > o.a_min) {
-            if (!both)
-              state = kGuideLo;
-            else if (account(outs[1]))
-              fallback();
-            else
-              refine();
+          } else if (lo_chk && !packed) {
+            state = kGuideLo;
+          } else if (lo_chk && account(outs[1])) {
+            fallback();
           } else {
             refine();
+            // the refinement levels this round ran speculatively, in order
+            const int k0 = lo_chk ? 2 : 1;
+            int node = 0;
+            for (int d = 0; d < spec; d++) {
+              const double mid = sqrt(lo * hi);
+              const bool c = account(outs[k0 + node]);
+              if (c)
+                hi = mid;
+              else
+                lo = mid;
+              it++;
+              node = 2 * node + (c ? 1 : 2);
+            }
           }
         } else {  // kGuideLo
           if (account(outs[0]))
