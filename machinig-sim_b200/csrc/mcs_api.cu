@@ -333,6 +333,7 @@ struct Bucket {
 
 struct mcs_ctx {
   int device = 0;
+  mcs_plan* solve_scratch = nullptr;  // mcs_solve's plan, reused so calls allocate nothing new
   int sms = 0;
   int prio_low = 0, prio_high = 0;  // stream priority range (lower value = scheduled first)
   cudaStream_t stream = nullptr;
@@ -565,7 +566,8 @@ int upload2(mcs_ctx* ctx, cudaStream_t stream, void* d1, const void* h1, size_t 
 int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
                size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* o,
                bool capture, cudaStream_t stream, mcs_plan** out,
-               mcs_surrogate* sur = nullptr, const mcs_guide_opts* g = nullptr) {
+               mcs_surrogate* sur = nullptr, const mcs_guide_opts* g = nullptr,
+               mcs_plan* reuse = nullptr) {
   int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
   if (rc) return rc;
   if (sur && (!g || !(g->z > 0) || !(g->hw_min > 0) || !(g->hw_max >= g->hw_min) ||
@@ -588,7 +590,19 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
     grps[i] = pr.pp.groups > 1 ? 1 : 0;
     cost[i] = pr.cost;
   }
-  mcs_plan* pl = new mcs_plan();
+  // a reused plan keeps its device buffers (they only grow) and drops everything else
+  mcs_plan* pl = reuse ? reuse : new mcs_plan();
+  if (reuse) {
+    pl->n = 0;
+    pl->trials = false;
+    pl->sur = nullptr;
+    pl->buckets.clear();
+    pl->max_modes = pl->max_slots = 1;
+    pl->executed = false;
+  }
+  auto discard = [&](mcs_plan* q) {
+    if (q != reuse) plan_free(q);
+  };
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
@@ -596,7 +610,7 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
                     o->max_buckets, order,
                     pl->buckets);
   if (rc) {
-    plan_free(pl);
+    discard(pl);
     return rc;
   }
   const size_t nb = std::max<size_t>(1, pl->buckets.size());
@@ -604,14 +618,14 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
       (rc = pl->order.ensure(sizeof(int32_t) * std::max<size_t>(1, n_points))) ||
       (rc = pl->results.ensure(sizeof(mcs_result) * std::max<size_t>(1, n_points))) ||
       (rc = pl->queues.ensure(sizeof(unsigned int) * nb))) {
-    plan_free(pl);
+    discard(pl);
     return rc;
   }
   if (n_points) {
     rc = upload2(ctx, stream, pl->params.p, pp.data(), sizeof(PointParams) * n_points,
                  pl->order.p, order.data(), sizeof(int32_t) * n_points);
     if (rc) {
-      plan_free(pl);
+      discard(pl);
       return rc;
     }
   }
@@ -633,21 +647,21 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
         (rc = pl->guide.ensure(sizeof(float2) * n_points)) ||
         (rc = pl->ginfo.ensure(sizeof(mcs_guide_info) * n_points)) ||
         (rc = surrogate_reserve(sur))) {
-      plan_free(pl);
+      discard(pl);
       return rc;
     }
     cudaError_t e = cudaMemcpyAsync(pl->feat.p, f.data(), sizeof(float) * f.size(),
                                     cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) {
-      plan_free(pl);
+      discard(pl);
       return fail(MCS_ERR_CUDA, "feature upload failed: %s", cudaGetErrorString(e));
     }
   }
   if (capture) {
     cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) {
-      plan_free(pl);
+      discard(pl);
       return fail(MCS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
     }
     rc = enqueue(pl, stream, o, nullptr, nullptr, o->chatter_idx, /*with_guide=*/false);
@@ -655,13 +669,13 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
     e = cudaStreamEndCapture(stream, &g);
     if (rc || e != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
-      plan_free(pl);
+      discard(pl);
       return rc ? rc : fail(MCS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
     }
     pl->graph = g;
     e = cudaGraphInstantiate(&pl->exec, g, 0);
     if (e != cudaSuccess) {
-      plan_free(pl);
+      discard(pl);
       return fail(MCS_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
     }
   }
@@ -732,6 +746,7 @@ int mcs_destroy(mcs_ctx* c) {
   if (!c) return MCS_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  plan_free(c->solve_scratch);
   for (int b = 0; b < kMaxBuckets; b++) {
     if (c->aux[b]) cudaStreamDestroy(c->aux[b]);
     if (c->join[b]) cudaEventDestroy(c->join[b]);
@@ -897,8 +912,11 @@ int mcs_solve(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_mo
   std::lock_guard<std::mutex> lk(c->mu);
   MCS_CUDA(cudaSetDevice(c->device));
   mcs_plan* pl = nullptr;
+  // the context's solve plan is reused: its device buffers persist between calls, so a
+  // repeated solve of a similar batch neither allocates nor frees device memory
+  if (!c->solve_scratch) c->solve_scratch = new mcs_plan();
   int rc = build_plan(c, setups, n_setups, modals, n_modals, points, n_points, opts, false,
-                      c->stream, &pl);
+                      c->stream, &pl, nullptr, nullptr, c->solve_scratch);
   if (rc) return rc;
   rc = enqueue(pl, c->stream, opts, nullptr, nullptr, opts->chatter_idx);
   if (!rc && n_points) {
@@ -908,7 +926,6 @@ int mcs_solve(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_mo
   }
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "solve failed: %s", cudaGetErrorString(e));
-  plan_free(pl);
   return rc;
 }
 
