@@ -333,7 +333,8 @@ struct Bucket {
 
 struct mcs_ctx {
   int device = 0;
-  mcs_plan* solve_scratch = nullptr;  // mcs_solve's plan, reused so calls allocate nothing new
+  mcs_plan* solve_scratch = nullptr;   // mcs_solve's plan, reused so calls allocate nothing new
+  mcs_plan* guided_scratch = nullptr;  // mcs_solve_guided's plan, likewise
   int sms = 0;
   int prio_low = 0, prio_high = 0;  // stream priority range (lower value = scheduled first)
   cudaStream_t stream = nullptr;
@@ -601,7 +602,12 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
     pl->executed = false;
   }
   auto discard = [&](mcs_plan* q) {
-    if (q != reuse) plan_free(q);
+    if (q != reuse) {
+      plan_free(q);
+    } else if (q->sur) {  // a reused plan keeps its buffers but not the surrogate
+      surrogate_hold(q->sur, -1);
+      q->sur = nullptr;
+    }
   };
   pl->ctx = ctx;
   pl->n = n_points;
@@ -747,6 +753,7 @@ int mcs_destroy(mcs_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   plan_free(c->solve_scratch);
+  plan_free(c->guided_scratch);
   for (int b = 0; b < kMaxBuckets; b++) {
     if (c->aux[b]) cudaStreamDestroy(c->aux[b]);
     if (c->join[b]) cudaEventDestroy(c->join[b]);
@@ -1134,9 +1141,11 @@ int mcs_solve_guided(mcs_ctx* c, mcs_surrogate* sur, const mcs_setup* setups, si
   std::lock_guard<std::mutex> lk(c->mu);
   std::lock_guard<std::mutex> slk(surrogate_mutex(sur));
   MCS_CUDA(cudaSetDevice(c->device));
+  // the context's guided plan is reused like mcs_solve's: no device allocation per call
+  if (!c->guided_scratch) c->guided_scratch = new mcs_plan();
   mcs_plan* pl = nullptr;
   int rc = build_plan(c, setups, n_setups, modals, n_modals, points, n_points, opts, false,
-                      c->stream, &pl, sur, g);
+                      c->stream, &pl, sur, g, c->guided_scratch);
   if (rc) return rc;
   rc = enqueue(pl, c->stream, opts, nullptr, nullptr, opts->chatter_idx);
   if (!rc && n_points) {
@@ -1150,7 +1159,10 @@ int mcs_solve_guided(mcs_ctx* c, mcs_surrogate* sur, const mcs_setup* setups, si
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "guided solve failed: %s", cudaGetErrorString(e));
   if (!rc) rc = surrogate_check(sur);
-  plan_free(pl);
+  if (pl->sur) {  // the plan is kept for the next call; the surrogate is not held by it
+    surrogate_hold(pl->sur, -1);
+    pl->sur = nullptr;
+  }
   return rc;
 }
 
