@@ -25,7 +25,7 @@ from . import _abi as A
 from ._lib import Context
 
 CACHE = Path(__file__).resolve().parent.parent / "tune_cache.json"
-CANDIDATES = (4, 8, 16, 24, 32)
+CANDIDATES = (3, 4, 6, 8, 12, 16, 24, 32)
 _LOCK = threading.Lock()
 
 
