@@ -211,10 +211,11 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
   // whose engaged window starts at position p0 is in cut when j_i = (pr + i*spt - p0) mod
   // spr < len.  With q = (pr - p0) mod spr = c*spt + r, j_i = ((c + i) mod N)*spt + r: the
   // teeth in cut at a step are those with u = (c + i) mod N < U, U = ceil((len - r)/spt),
-  // so a lane visits only its own in-cut teeth, in rounds u = 0, 1, ...
+  // so a lane visits only its own in-cut teeth, in rounds u = 0, 1, ...  The tooth of round
+  // u is i = (u - c) mod N = tb + u with tb = (N - c) mod N: i < 2N, no wrap.
   T sL[SLOTS], cL[SLOTS], ktb[SLOTS], kteb[SLOTS], krb[SLOTS], kreb[SLOTS], pdc[SLOTS],
       fzk[SLOTS];
-  int p0[SLOTS], len[SLOTS], base[SLOTS], cph[SLOTS], rph[SLOTS];
+  int p0[SLOTS], len[SLOTS], base[SLOTS], tb[SLOTS], rph[SLOTS];
 #pragma unroll
   for (int s = 0; s < SLOTS; s++) {
     const int k = ll + gs * s;  // slice; its ring row is the lane's own
@@ -257,8 +258,9 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
       fzk[s] = (T)(P->fz * kap);
     }
     const int q = (spr - p0[s]) % spr;  // phase at pr = 0
-    cph[s] = q / spt;
-    rph[s] = q - cph[s] * spt;
+    const int c = q / spt;
+    rph[s] = q - c * spt;
+    tb[s] = c == 0 ? 0 : N - c;
   }
   // a fresh engine's surface is all zeros (cutting.js:68): the trial's rows
   if (GR) {
@@ -276,8 +278,8 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
   for (int s = 0; s < SLOTS; s++) maxlen = max(maxlen, len[s]);
   const int rounds = min(N, (__reduce_max_sync(kFull, (unsigned)maxlen) + spt - 1) / spt);
 
-  // lane i < N holds tooth i's runout offset (read by shuffle)
-  const T dRl = lane < kMaxTeeth ? (T)P->dR[lane] : T(0);
+  // lane i < 2N holds the runout offset of tooth i mod N (read by shuffle; N <= 8)
+  const T dRl = lane < 2 * N ? (T)P->dR[lane < N ? lane : lane - N] : T(0);
   // Modal state.  Linear cuts split it: the group's lower half integrates the x modes and
   // its upper half the y modes (row 0 holds this half's axis), which halves the update and
   // the force sum at the price of a broadcast of x and y on the step's critical path.  With
@@ -334,9 +336,7 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
       if (!__any_sync(kFull, any)) break;  // rounds are monotone: later ones are empty too
 #pragma unroll
       for (int s = 0; s < SLOTS; s++) {
-        int i = u - cph[s];
-        if (i < 0) i += N;
-        const T dRi = __shfl_sync(kFull, dRl, i);
+        const T dRi = __shfl_sync(kFull, dRl, tb[s] + u);  // u < rounds <= N
         // idle lanes (no in-cut tooth this round, or a slice past nz whose ring row is not
         // this trial's) read a valid table entry and neither read nor write the ring
         const int j = act[s] ? jj[s] : 0;
@@ -405,9 +405,9 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
     // the revolution advances one position: every slot's phase follows
 #pragma unroll
     for (int s = 0; s < SLOTS; s++) {
-      if (++rph[s] == spt) {
+      if (++rph[s] == spt) {  // c advances, so tb = (N - c) mod N goes back
         rph[s] = 0;
-        if (++cph[s] == N) cph[s] = 0;
+        tb[s] = tb[s] == 0 ? N - 1 : tb[s] - 1;
       }
     }
     if (++phc == spt) {  // once-per-tooth sample (cutting.js:266-268), Float32Array
