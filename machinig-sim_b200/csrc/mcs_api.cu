@@ -338,10 +338,7 @@ struct mcs_ctx {
   int sms = 0;
   int prio_low = 0, prio_high = 0;  // stream priority range (lower value = scheduled first)
   cudaStream_t stream = nullptr;
-  cudaStream_t aux[kMaxBuckets] = {};
   cudaStream_t side = nullptr;  // progress reads and cancellation while a job runs
-  cudaEvent_t fork = nullptr;
-  cudaEvent_t join[kMaxBuckets] = {};
   std::mutex mu;
   void* pinned = nullptr;  // upload staging (page-locked), grown on demand
   size_t pinned_cap = 0;
@@ -463,11 +460,13 @@ int enqueue_guide(mcs_plan* pl, cudaStream_t s0) {
 }
 
 // Enqueue the plan's work: zero the queue counters, (optionally) the surrogate's
-// predictions, then fork one stream per bucket and join.  Captured plans leave the
-// predictions out of the graph and run them just before it (mcs_plan_execute): with the
-// inference kernel inside the graph, ahead of the fork, the same bucket kernels ran 7 %
-// slower on 65536 serving queries (a graph's start order of parallel branches is not
-// specified).
+// predictions, then the buckets as one chain of programmatic dependent launches on the
+// same stream, longest points first: each bucket's kernel starts once every block of the
+// one before is resident, so the long points always take the SMs first (parallel graph
+// branches, one per bucket, started in an unspecified order: the sweep ran 204 or 242 ms
+// from one execution to the next).  Captured plans leave the predictions out of the graph
+// and run them just before it (mcs_plan_execute): with the inference kernel inside the
+// graph the same bucket kernels ran 7 % slower on 65536 serving queries.
 int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int* cancel,
             unsigned int* progress, double chatter_idx, bool with_guide = true) {
   mcs_ctx* ctx = pl->ctx;
@@ -487,33 +486,28 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
     ga.hw_min = pl->gopts.hw_min;
     ga.refine = pl->gopts.refine;
   }
-  MCS_CUDA(cudaEventRecord(ctx->fork, s0));
   for (int b = 0; b < nb; b++) {
     const Bucket& bk = pl->buckets[b];
-    cudaStream_t sb = nb == 1 ? s0 : ctx->aux[b];
-    if (sb != s0) MCS_CUDA(cudaStreamWaitEvent(sb, ctx->fork, 0));
+    const bool chained = b > 0;  // the first waits for the memsets and the predictions
     unsigned int* q = static_cast<unsigned int*>(pl->queues.p) + b;
     const int32_t* order = static_cast<const int32_t*>(pl->order.p) + bk.offset;
     int rc;
-    // buckets come in decreasing shared-memory need, i.e. longest points first: they get
-    // the highest priority, so their warps start before the short points fill the SMs
+    // buckets come in decreasing shared-memory need, i.e. longest points first; they also
+    // get decreasing block priorities for the SMs that free up while several run
     const int prio = std::min(ctx->prio_low, ctx->prio_high + b);
     if (pl->trials)
-      rc = launch_trials(bk.shape, bk.grid, bk.smem, sb,
+      rc = launch_trials(bk.shape, bk.grid, bk.smem, s0,
                          static_cast<const PointParams*>(pl->params.p),
                          static_cast<const TrialItem*>(pl->items.p) + bk.offset, bk.count,
-                         chatter_idx, static_cast<mcs_trial_result*>(pl->results.p), q, prio);
+                         chatter_idx, static_cast<mcs_trial_result*>(pl->results.p), q, prio,
+                         chained);
     else
-      rc = launch_solve(bk.shape, bk.grid, bk.smem, sb,
+      rc = launch_solve(bk.shape, bk.grid, bk.smem, s0,
                         static_cast<const PointParams*>(pl->params.p), order, bk.count,
                         dev_opts(o), static_cast<mcs_result*>(pl->results.p), q, cancel,
-                        progress, ga, prio);
+                        progress, ga, prio, chained);
     if (rc != 0)
       return fail(MCS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString((cudaError_t)rc));
-    if (sb != s0) {
-      MCS_CUDA(cudaEventRecord(ctx->join[b], sb));
-      MCS_CUDA(cudaStreamWaitEvent(s0, ctx->join[b], 0));
-    }
   }
   return MCS_OK;
 }
@@ -734,12 +728,8 @@ int mcs_create(mcs_ctx** out, int device) {
   c->device = device;
   c->sms = prop.multiProcessorCount;
   MCS_CUDA(cudaDeviceGetStreamPriorityRange(&c->prio_low, &c->prio_high));
-  bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
-  for (int b = 0; ok && b < kMaxBuckets; b++)
-    ok = cudaStreamCreateWithFlags(&c->aux[b], cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreateWithFlags(&c->join[b], cudaEventDisableTiming) == cudaSuccess;
+  const bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess;
   if (!ok) {
     mcs_destroy(c);
     return fail(MCS_ERR_CUDA, "stream/event creation failed");
@@ -754,11 +744,6 @@ int mcs_destroy(mcs_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   plan_free(c->solve_scratch);
   plan_free(c->guided_scratch);
-  for (int b = 0; b < kMaxBuckets; b++) {
-    if (c->aux[b]) cudaStreamDestroy(c->aux[b]);
-    if (c->join[b]) cudaEventDestroy(c->join[b]);
-  }
-  if (c->fork) cudaEventDestroy(c->fork);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->pinned) cudaFreeHost(c->pinned);

@@ -119,15 +119,19 @@ struct KernelShape {
   int grouped = 0;  // 1: points may run several trials per warp in lane groups
 };
 
-// Host launchers (mcs_kernels.cu).
+// Host launchers (mcs_kernels.cu).  chained = 1: a programmatic dependent launch behind the
+// previous kernel of the stream (the previous bucket of a plan), which it may overlap once
+// all of that kernel's blocks are resident, and whose completion its own completion
+// implies.
 int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                  const PointParams* pts, const int32_t* order, int n, DevOpts opts,
                  mcs_result* out, unsigned int* queue, const volatile int* cancel,
                  unsigned int* progress, const GuideArgs& guide = GuideArgs(),
-                 int priority = 0);
+                 int priority = 0, bool chained = false);
 int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                   const PointParams* pts, const TrialItem* items, int n, double chatter_idx,
-                  mcs_trial_result* out, unsigned int* queue, int priority = 0);
+                  mcs_trial_result* out, unsigned int* queue, int priority = 0,
+                  bool chained = false);
 int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm);
 int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm);
 int set_smem_limits();

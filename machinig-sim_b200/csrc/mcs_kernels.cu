@@ -338,7 +338,8 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
       for (int s = 0; s < SLOTS; s++) {
         const T dRi = __shfl_sync(kFull, dRl, tb[s] + u);  // u < rounds <= N
         // idle lanes (no in-cut tooth this round, or a slice past nz whose ring row is not
-        // this trial's) read a valid table entry and neither read nor write the ring
+        // this trial's) read a valid table entry, take their surface word from the table
+        // (read-only here; the value is discarded) and never write the ring
         const int j = act[s] ? jj[s] : 0;
         int p = p0[s] + j;  // table position of tooth i at this step (p0 < spr, j < spr)
         if (p >= spr) p -= spr;
@@ -348,8 +349,9 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
         const T cs = A::madd(sc.y, cL[s], sc.x * sL[s]);
         // feed u = [1, 0]: edge normal n = (sin phi, cos phi), tangent t = (cos, -sin)
         const T rn = A::madd(xm, sn, A::madd(ym, cs, dRi));
-        float* cell = ring + (act[s] ? base[s] + j : 0);
-        const T prev = act[s] ? (T)*cell : T(0);
+        float* cell = ring + base[s] + j;
+        const float* src = act[s] ? cell : reinterpret_cast<const float*>(table);
+        const T prev = (T)*src;
         const T feedH = fzk[s] * sn;
         T h = (feedH + rn) - prev;
         const bool cut = h > T(0);
@@ -588,6 +590,19 @@ __device__ __forceinline__ TrialOut simulate_trial(const PointParams* __restrict
   return out[0];
 }
 
+// The buckets of a plan run as a chain of programmatic dependent launches on one stream.
+// chain_start: this block is resident, so the next bucket's kernel may launch once every
+// block of this one has said so (a no-op when nothing is chained behind).  chain_end:
+// block 0 waits, before it exits, for the previous bucket's kernel to complete, so the
+// completion of the last bucket implies that of all; the previous kernel's blocks are all
+// resident by then and depend on nothing later, so the wait ends (a no-op for the first).
+__device__ __forceinline__ void chain_start() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void chain_end() {
+  if (blockIdx.x == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane) {
   int c = 0;
   if (cancel != nullptr && lane == 0) c = *cancel;
@@ -604,6 +619,7 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
                                                       unsigned int* progress, GuideArgs g) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x;
+  chain_start();
   for (;;) {
     unsigned int w = 0;
     if (lane == 0) w = atomicAdd(queue, 1u);
@@ -826,6 +842,7 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
     }
     __syncwarp();
   }
+  chain_end();
 }
 
 // Batch of independent chatterAt trials (decision replay at given depths).
@@ -837,6 +854,7 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) trials_kernel(const
                                                        unsigned int* __restrict__ queue) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x;
+  chain_start();
   for (;;) {
     unsigned int w = 0;
     if (lane == 0) w = atomicAdd(queue, 1u);
@@ -865,6 +883,7 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) trials_kernel(const
     }
     __syncwarp();
   }
+  chain_end();
 }
 
 template <typename T, int SLOTS, int NM>
@@ -930,41 +949,45 @@ int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm) {
   return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, kWarp, smem);
 }
 
-// One-warp blocks with a scheduling priority (lower value = scheduled first), so that the
-// buckets of long points get their SMs before the buckets of short ones fill the device.
+// One-warp blocks with a scheduling priority (lower value = scheduled first).  A chained
+// launch is a programmatic dependent launch: it may start once every block of the
+// stream's previous kernel has started (chain_start), so the buckets of a plan take the
+// SMs in the order they are launched, longest points first.
 int launch_with_priority(void* f, int grid, int smem, cudaStream_t stream, void** args,
-                         int priority) {
+                         int priority, bool chained) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kWarp);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributePriority;
   attr[0].val.priority = priority;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = chained ? 2 : 1;
   return (int)cudaLaunchKernelExC(&cfg, f, args);
 }
 
 int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                  const PointParams* pts, const int32_t* order, int n, DevOpts opts,
                  mcs_result* out, unsigned int* queue, const volatile int* cancel,
-                 unsigned int* progress, const GuideArgs& guide, int priority) {
+                 unsigned int* progress, const GuideArgs& guide, int priority, bool chained) {
   void* f = pick(true, shape);
   if (!f) return (int)cudaErrorInvalidValue;
   GuideArgs g = guide;
   void* args[] = {&pts, &order, &n, &opts, &out, &queue, &cancel, &progress, &g};
-  return launch_with_priority(f, grid, smem, stream, args, priority);
+  return launch_with_priority(f, grid, smem, stream, args, priority, chained);
 }
 
 int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
                   const PointParams* pts, const TrialItem* items, int n, double chatter_idx,
-                  mcs_trial_result* out, unsigned int* queue, int priority) {
+                  mcs_trial_result* out, unsigned int* queue, int priority, bool chained) {
   void* f = pick(false, shape);
   if (!f) return (int)cudaErrorInvalidValue;
   void* args[] = {&pts, &items, &n, &chatter_idx, &out, &queue};
-  return launch_with_priority(f, grid, smem, stream, args, priority);
+  return launch_with_priority(f, grid, smem, stream, args, priority, chained);
 }
 
 }  // namespace mcs
