@@ -338,7 +338,10 @@ struct mcs_ctx {
   int sms = 0;
   int prio_low = 0, prio_high = 0;  // stream priority range (lower value = scheduled first)
   cudaStream_t stream = nullptr;
+  cudaStream_t aux[kMaxBuckets] = {};  // one per bucket for direct (uncaptured) calls
   cudaStream_t side = nullptr;  // progress reads and cancellation while a job runs
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kMaxBuckets] = {};
   std::mutex mu;
   void* pinned = nullptr;  // upload staging (page-locked), grown on demand
   size_t pinned_cap = 0;
@@ -460,15 +463,21 @@ int enqueue_guide(mcs_plan* pl, cudaStream_t s0) {
 }
 
 // Enqueue the plan's work: zero the queue counters, (optionally) the surrogate's
-// predictions, then the buckets as one chain of programmatic dependent launches on the
-// same stream, longest points first: each bucket's kernel starts once every block of the
-// one before is resident, so the long points always take the SMs first (parallel graph
-// branches, one per bucket, started in an unspecified order: the sweep ran 204 or 242 ms
-// from one execution to the next).  Captured plans leave the predictions out of the graph
-// and run them just before it (mcs_plan_execute): with the inference kernel inside the
-// graph the same bucket kernels ran 7 % slower on 65536 serving queries.
+// predictions, then the buckets, longest points first.
+//  - Captured (a plan's graph): one chain of programmatic dependent launches on the same
+//    stream.  Each bucket's kernel starts once every block of the one before is resident,
+//    so the long points always take the SMs first.  Parallel graph branches, one per
+//    bucket, start in an unspecified order: the sweep ran 204 or 243 ms from one
+//    execution to the next.
+//  - Direct calls: one stream per bucket, forked and joined; the launches reach the device
+//    in issue order.  A chain of more than 8 dependent launches outside a graph ran the
+//    sweep in 309 ms instead of 199 ms.
+// Captured plans leave the predictions out of the graph and run them just before it
+// (mcs_plan_execute): with the inference kernel inside the graph the same bucket kernels
+// ran 7 % slower on 65536 serving queries.
 int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int* cancel,
-            unsigned int* progress, double chatter_idx, bool with_guide = true) {
+            unsigned int* progress, double chatter_idx, bool with_guide = true,
+            bool captured = false) {
   mcs_ctx* ctx = pl->ctx;
   const int nb = (int)pl->buckets.size();
   MCS_CUDA(cudaMemsetAsync(pl->queues.p, 0, sizeof(unsigned int) * std::max(1, nb), s0));
@@ -486,9 +495,14 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
     ga.hw_min = pl->gopts.hw_min;
     ga.refine = pl->gopts.refine;
   }
+  const bool forked = !captured && nb > 1;
+  if (forked) MCS_CUDA(cudaEventRecord(ctx->fork, s0));
   for (int b = 0; b < nb; b++) {
     const Bucket& bk = pl->buckets[b];
-    const bool chained = b > 0;  // the first waits for the memsets and the predictions
+    // the first bucket waits for the memsets and the predictions like any stream work
+    const bool chained = captured && b > 0;
+    cudaStream_t sb = forked ? ctx->aux[b] : s0;
+    if (forked) MCS_CUDA(cudaStreamWaitEvent(sb, ctx->fork, 0));
     unsigned int* q = static_cast<unsigned int*>(pl->queues.p) + b;
     const int32_t* order = static_cast<const int32_t*>(pl->order.p) + bk.offset;
     int rc;
@@ -496,18 +510,22 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
     // get decreasing block priorities for the SMs that free up while several run
     const int prio = std::min(ctx->prio_low, ctx->prio_high + b);
     if (pl->trials)
-      rc = launch_trials(bk.shape, bk.grid, bk.smem, s0,
+      rc = launch_trials(bk.shape, bk.grid, bk.smem, sb,
                          static_cast<const PointParams*>(pl->params.p),
                          static_cast<const TrialItem*>(pl->items.p) + bk.offset, bk.count,
                          chatter_idx, static_cast<mcs_trial_result*>(pl->results.p), q, prio,
                          chained);
     else
-      rc = launch_solve(bk.shape, bk.grid, bk.smem, s0,
+      rc = launch_solve(bk.shape, bk.grid, bk.smem, sb,
                         static_cast<const PointParams*>(pl->params.p), order, bk.count,
                         dev_opts(o), static_cast<mcs_result*>(pl->results.p), q, cancel,
                         progress, ga, prio, chained);
     if (rc != 0)
       return fail(MCS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+    if (forked) {
+      MCS_CUDA(cudaEventRecord(ctx->join[b], sb));
+      MCS_CUDA(cudaStreamWaitEvent(s0, ctx->join[b], 0));
+    }
   }
   return MCS_OK;
 }
@@ -664,7 +682,8 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
       discard(pl);
       return fail(MCS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
     }
-    rc = enqueue(pl, stream, o, nullptr, nullptr, o->chatter_idx, /*with_guide=*/false);
+    rc = enqueue(pl, stream, o, nullptr, nullptr, o->chatter_idx, /*with_guide=*/false,
+                 /*captured=*/true);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(stream, &g);
     if (rc || e != cudaSuccess) {
@@ -728,8 +747,12 @@ int mcs_create(mcs_ctx** out, int device) {
   c->device = device;
   c->sms = prop.multiProcessorCount;
   MCS_CUDA(cudaDeviceGetStreamPriorityRange(&c->prio_low, &c->prio_high));
-  const bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
-                  cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess;
+  bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int b = 0; ok && b < kMaxBuckets; b++)
+    ok = cudaStreamCreateWithFlags(&c->aux[b], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->join[b], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     mcs_destroy(c);
     return fail(MCS_ERR_CUDA, "stream/event creation failed");
@@ -744,6 +767,11 @@ int mcs_destroy(mcs_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   plan_free(c->solve_scratch);
   plan_free(c->guided_scratch);
+  for (int b = 0; b < kMaxBuckets; b++) {
+    if (c->aux[b]) cudaStreamDestroy(c->aux[b]);
+    if (c->join[b]) cudaEventDestroy(c->join[b]);
+  }
+  if (c->fork) cudaEventDestroy(c->fork);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->pinned) cudaFreeHost(c->pinned);
