@@ -9,6 +9,8 @@ pytestmark = pytest.mark.gpu
 
 
 def test_results_identical_for_every_schedule(ctx):
+    # the direct call forks one stream per bucket; the plan's graph chains the buckets as
+    # programmatic dependent launches: both launch paths, at up to 32 buckets
     from mcs import _abi as A
     from mcs import workloads as W
 
