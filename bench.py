@@ -48,6 +48,11 @@ METRIC = "stability-boundary points/sec on 1 B200: surrogate-guided vs plain GPU
 UNIT = "points/s"
 FLOP_ENGAGED = 46.0   # FP32 flop per in-cut slice evaluation (force law, cutting.js:181-207)
 FLOP_IDLE = 15.0      # per out-of-cut evaluation of the reference loop (angle, normal, store)
+# DRAM bytes per point of one solve, from an ncu capture of a 3072-point sweep (FP32, 8
+# buckets): dram__bytes.sum.per_second x gpu__time_duration of each bucket launch, summed,
+# 4.63 MB per execution.  A point reads its parameters and writes its result once; the
+# trial state lives in registers and shared memory, so the bytes scale with the points.
+DRAM_BYTES_PER_POINT = {"sweep": 1508.0}
 
 
 def env_rank():
@@ -441,7 +446,11 @@ def ours(args) -> int:
                        "schedule": info["schedule"]},
             "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops,
                          "unit": "TFLOP/s", "frac": achieved_tflops / peak_tflops,
-                         "traffic": None,
+                         "traffic": (DRAM_BYTES_PER_POINT[args.workload] * wl.n
+                                     if args.workload in DRAM_BYTES_PER_POINT
+                                     and args.precision == "fp32" else None),
+                         "traffic_unit": "bytes per step, scaled by points from an ncu "
+                                         "capture of a 3072-point FP32 sweep",
                          "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 flop x "
                                         f"{f_mhz:.0f} MHz sampled SM clock (no FP32 figure "
                                         "in MEASURED_PEAKS.json)",
