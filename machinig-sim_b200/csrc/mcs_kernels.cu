@@ -63,6 +63,10 @@ struct Arith<float> {
   static __device__ __forceinline__ float2 pair(double s, double c) {
     return make_float2((float)s, (float)c);
   }
+  // the history's Float32Array sample of a position [m] in um (cutting.js:288-292): the
+  // product of a float and 1e6 is exact in double, so rounding it to float gives the
+  // correctly rounded float product
+  static __device__ __forceinline__ float micro(float v) { return v * 1e6f; }
 };
 template <>
 struct Arith<double> {
@@ -72,6 +76,7 @@ struct Arith<double> {
     return h * pow(0.05 / (h > 0.002 ? h : 0.002), mc);
   }
   static __device__ __forceinline__ double2 pair(double s, double c) { return make_double2(s, c); }
+  static __device__ __forceinline__ float micro(double v) { return (float)(v * 1e6); }
 };
 
 // Resident warps per SM the register allocation is held to (65536 / (32 * warps)); measured
@@ -309,7 +314,7 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
   const int nsteps = P->nsteps, decim = P->decim, ts_c0 = P->ts_c0, h0 = P->hist_h0;
   const int n_ts = P->ts_n;
   int phc = 0, dcnt = 0, tcount = 0, hcount = 0, eng = 0;
-  float shx = 0.f, shy = 0.f;
+  double sh = 0.0;  // first history sample in the window of this lane's axis
   float tsx = 0.f, tsy = 0.f;  // without groups lane t keeps tooth sample t
   // FP64 sums of the history window.  Without groups one per lane of lanes 0-3: sum dx,
   // sum dy, sum dx^2, sum dy^2.  In lane groups (as small as 2 lanes) two per lane of the
@@ -427,12 +432,10 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
     if (++dcnt == decim) {  // decimated history (cutting.js:288-292), FP64 window sums
       dcnt = 0;
       if (hcount >= h0) {
-        const float hx = (float)((double)x * 1e6), hy = (float)((double)y * 1e6);
-        if (hcount == h0) {
-          shx = hx;
-          shy = hy;
-        }
-        const double d = (ll & 1) ? (double)hy - (double)shy : (double)hx - (double)shx;
+        // lane bit 0 picks the axis: x on even lanes, y on odd ones
+        const double hv = (double)A::micro((ll & 1) ? y : x);
+        if (hcount == h0) sh = hv;
+        const double d = hv - sh;
         if (GR) {
           acc = acc + d;
           acc2 = fma(d, d, acc2);
