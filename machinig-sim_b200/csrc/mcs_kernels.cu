@@ -171,7 +171,7 @@ __device__ __forceinline__ T group_sum_xy(T fx, T fy, bool upper, int gs, int la
 }
 
 // The lane groups of one warp and the depth each simulates.  Groups are aligned blocks of
-// a power-of-two number of lanes (>= 4) that cover the warp; a group with ap = 0 has no
+// a power-of-two number of lanes (>= 2) that cover the warp; a group with ap = 0 has no
 // slices and its result is not used.
 struct Groups {
   int n;                    // groups
