@@ -243,20 +243,23 @@ void mcs_job_free(mcs_job* job);
 
 /*
  * Solve without allocating: the same batched timeDomainLimit as mcs_solve, for callers
- * that must not allocate GPU memory -- code that runs while a CUDA graph is being built
- * on another stream, real-time loops where the device-wide synchronisation of
- * cudaMalloc/cudaFree would stall other work, or hosts whose device memory is owned by
- * another allocator.  This entry point has no counterpart in the reference.
+ * that must not allocate GPU memory.  Such callers are real-time loops (a machine-side
+ * monitor that re-checks a few speeds per tick), where cudaMalloc/cudaFree may
+ * synchronise the whole device and stall the loop, and host applications whose device
+ * memory is already claimed by their own allocator or held to a fixed budget, where an
+ * allocation in the middle of a run can fail with out-of-memory.  This entry point has
+ * no counterpart in the reference.
  *
  * Inputs and outputs are the caller's host arrays, as for mcs_solve.  The per-point
  * parameters, the work queue and the device copy of the results live in a preallocated
  * scratch area that every GPU loading the library holds until the process exits
  * (about 0.5 MB), so a call solves at most MCS_NOALLOC_MAX_POINTS points; larger batches
- * fail with MCS_ERR_ARG.  The first call on a device looks the scratch area up (make it
- * before any stream capture).  All calls share the area: the library serialises them
- * per device and each call waits for its work, so its calls never overlap on the GPU;
- * work that touched the area concurrently would race.  It calls no cudaMalloc, cudaFree
- * or other allocating routine.
+ * fail with MCS_ERR_ARG.  The first call on a device looks the scratch area's device
+ * address up; make that first call before any stream capture.  All calls share the area
+ * and it keeps the last call's contents: the library serialises the calls per device and
+ * every call, also one that fails, waits for its own copies and kernels before it
+ * returns, so its calls never overlap on the GPU; work that touched the area at the same
+ * time would race.  It calls no cudaMalloc, cudaFree or other allocating routine.
  */
 #define MCS_NOALLOC_MAX_POINTS 1024
 int mcs_solve_noalloc(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups,

@@ -1333,52 +1333,62 @@ extern "C" int mcs_solve_noalloc(mcs_ctx* c, const mcs_setup* setups, size_t n_s
   auto* d_params = reinterpret_cast<PointParams*>(base + kNaParamsOff);
   auto* d_results = reinterpret_cast<mcs_result*>(base + kNaResultsOff);
 
-  // prepare on the host in stack-sized chunks and copy each into the scratch area
-  PointParams chunk[kNaChunk];
-  double cost[kNaMax];
-  int32_t order[kNaMax];
-  int smem = 0, slots = 1, modes = 1, nl = 0, gr = 0;
-  for (size_t i0 = 0; i0 < n_points; i0 += kNaChunk) {
-    const size_t m = std::min<size_t>(kNaChunk, n_points - i0);
-    for (size_t j = 0; j < m; j++) {
-      const size_t i = i0 + j;
-      Prepared pr;
-      rc = prepare_point(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,
-                         o->a_max, pr);
-      if (rc) return fail(rc, "point %zu: %s", i, g_last_error.c_str());
-      chunk[j] = pr.pp;
-      cost[i] = pr.cost;
-      smem = std::max(smem, pr.pp.smem_bytes);
-      slots = std::max(slots, slots_for(pr.pp.nz_max));
-      modes = std::max(modes, pr.modes);
-      nl = std::max(nl, pr.nl);
-      gr = std::max(gr, pr.pp.groups > 1 ? 1 : 0);
+  // Everything that touches the scratch area; whatever it returns, the stream is drained
+  // below before the device lock is released, so that no copy or kernel of this call is
+  // still using the area when the next call starts, on this context or another.
+  auto body = [&]() -> int {
+    // prepare on the host in stack-sized chunks and copy each into the scratch area
+    PointParams chunk[kNaChunk];
+    double cost[kNaMax];
+    int32_t order[kNaMax];
+    int smem = 0, slots = 1, modes = 1, nl = 0, gr = 0;
+    for (size_t i0 = 0; i0 < n_points; i0 += kNaChunk) {
+      const size_t m = std::min<size_t>(kNaChunk, n_points - i0);
+      for (size_t j = 0; j < m; j++) {
+        const size_t i = i0 + j;
+        Prepared pr;
+        const int prc = prepare_point(setups[points[i].setup], modals[points[i].modal],
+                                      points[i].S, *o, o->a_max, pr);
+        if (prc) return fail(prc, "point %zu: %s", i, g_last_error.c_str());
+        chunk[j] = pr.pp;
+        cost[i] = pr.cost;
+        smem = std::max(smem, pr.pp.smem_bytes);
+        slots = std::max(slots, slots_for(pr.pp.nz_max));
+        modes = std::max(modes, pr.modes);
+        nl = std::max(nl, pr.nl);
+        gr = std::max(gr, pr.pp.groups > 1 ? 1 : 0);
+      }
+      MCS_CUDA(cudaMemcpyAsync(d_params + i0, chunk, sizeof(PointParams) * m,
+                               cudaMemcpyHostToDevice, st));
+      MCS_CUDA(cudaStreamSynchronize(st));  // the chunk buffer is reused
     }
-    MCS_CUDA(cudaMemcpyAsync(d_params + i0, chunk, sizeof(PointParams) * m,
+    // largest first, for the persistent warps' load balance
+    for (size_t i = 0; i < n_points; i++) order[i] = (int32_t)i;
+    std::sort(order, order + n_points, [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+    MCS_CUDA(cudaMemcpyAsync(d_order, order, sizeof(int32_t) * n_points,
                              cudaMemcpyHostToDevice, st));
-    MCS_CUDA(cudaStreamSynchronize(st));  // the chunk buffer is reused
-  }
-  // largest first, for the persistent warps' load balance
-  for (size_t i = 0; i < n_points; i++) order[i] = (int32_t)i;
-  std::sort(order, order + n_points, [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
-  MCS_CUDA(cudaMemcpyAsync(d_order, order, sizeof(int32_t) * n_points, cudaMemcpyHostToDevice,
-                           st));
-  // the queue counter must start at zero; the area keeps the previous call's contents
-  MCS_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
-  const KernelShape shape{slots, modes, o->precision == MCS_FP64 ? 1 : 0, nl, gr};
-  smem = (smem + 15) & ~15;
-  int bps = 0;
-  const int orc = occupancy_solve(shape, smem, &bps);
-  if (orc != 0)
-    return fail(MCS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString((cudaError_t)orc));
-  if (bps < 1) return fail(MCS_ERR_UNSUPPORTED, "a %d-byte warp does not fit on an SM", smem);
-  const int grid = (int)std::min<long long>((long long)n_points, (long long)bps * c->sms);
-  const int lrc = launch_solve(shape, grid, smem, st, d_params, d_order, (int)n_points,
-                               dev_opts(o), d_results, d_queue, nullptr, nullptr);
-  if (lrc != 0)
-    return fail(MCS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString((cudaError_t)lrc));
-  MCS_CUDA(cudaMemcpyAsync(out, d_results, sizeof(mcs_result) * n_points,
-                           cudaMemcpyDeviceToHost, st));
-  MCS_CUDA(cudaStreamSynchronize(st));
-  return MCS_OK;
+    // the queue counter must start at zero; the area keeps the previous call's contents
+    MCS_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned int), st));
+    const KernelShape shape{slots, modes, o->precision == MCS_FP64 ? 1 : 0, nl, gr};
+    smem = (smem + 15) & ~15;
+    int bps = 0;
+    const int orc = occupancy_solve(shape, smem, &bps);
+    if (orc != 0)
+      return fail(MCS_ERR_CUDA, "occupancy query failed: %s",
+                  cudaGetErrorString((cudaError_t)orc));
+    if (bps < 1) return fail(MCS_ERR_UNSUPPORTED, "a %d-byte warp does not fit on an SM", smem);
+    const int grid = (int)std::min<long long>((long long)n_points, (long long)bps * c->sms);
+    const int lrc = launch_solve(shape, grid, smem, st, d_params, d_order, (int)n_points,
+                                 dev_opts(o), d_results, d_queue, nullptr, nullptr);
+    if (lrc != 0)
+      return fail(MCS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString((cudaError_t)lrc));
+    MCS_CUDA(cudaMemcpyAsync(out, d_results, sizeof(mcs_result) * n_points,
+                             cudaMemcpyDeviceToHost, st));
+    return MCS_OK;
+  };
+  rc = body();
+  const cudaError_t e = cudaStreamSynchronize(st);
+  if (!rc && e != cudaSuccess)
+    rc = fail(MCS_ERR_CUDA, "allocation-free solve failed: %s", cudaGetErrorString(e));
+  return rc;
 }
