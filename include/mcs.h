@@ -371,6 +371,21 @@ int mcs_plan_create_guided(mcs_ctx* ctx, mcs_surrogate* s, const mcs_setup* setu
                            const mcs_guide_opts* g, mcs_plan** plan);
 int mcs_plan_guide_info(mcs_plan* plan, mcs_guide_info* info);
 
+/* ------------------------------------------------------------------ measurement
+ * Peak rates of the context's device, measured with CUDA events on its stream: FP32 and
+ * FP64 FMA issue (2 flop per FMA, every SM fully occupied) and shared-memory bandwidth
+ * (16-byte loads and stores at conflict-free addresses).  The solve kernels are bounded by
+ * these, not by HBM or tensor cores, so their roofline fractions are taken against these
+ * figures.  No counterpart in the reference.  Takes about a second; allocates a small
+ * device buffer for the call.
+ */
+typedef struct {
+  double fp32_tflops;
+  double fp64_tflops;
+  double smem_tbps; /* shared memory, TB/s summed over the SMs */
+} mcs_peaks;
+int mcs_measure_peaks(mcs_ctx* ctx, mcs_peaks* out);
+
 /*
  * Zero-order lobes (sld.js:23-61) read at spindle speeds (alimAt, sld.js:64-76):
  * alim[q * n_rpm + r] for query q at rpm[r]; +inf where no lobe covers the speed.

@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libmcs.so"
-SOURCES = ["mcs_kernels.cu", "mcs_lobes.cu", "mcs_surrogate.cu", "mcs_api.cu"]
+SOURCES = ["mcs_kernels.cu", "mcs_lobes.cu", "mcs_surrogate.cu", "mcs_probe.cu", "mcs_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -27,6 +27,16 @@ def nvcc() -> str:
     if not Path(cand).exists() and not shutil.which(cand):
         raise RuntimeError("nvcc not found")
     return cand
+
+
+BUILD = HERE / "_build"
+# (source, object, extra flags): the kernels file builds once per integration precision
+UNITS = [("mcs_kernels.cu", "mcs_kernels_f32.o", ["-DMCS_PREC=32"]),
+         ("mcs_kernels.cu", "mcs_kernels_f64.o", ["-DMCS_PREC=64"]),
+         ("mcs_lobes.cu", "mcs_lobes.o", []),
+         ("mcs_surrogate.cu", "mcs_surrogate.o", []),
+         ("mcs_probe.cu", "mcs_probe.o", []),
+         ("mcs_api.cu", "mcs_api.o", [])]
 
 
 def needs_build() -> bool:
@@ -38,17 +48,27 @@ def needs_build() -> bool:
 
 
 def build(verbose_ptxas: bool = False, force: bool = False) -> Path:
+    """Compile every unit to an object in parallel, then link libmcs.so."""
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-Wall", "--expt-relaxed-constexpr", "-I", str(ROOT / "include"),
-           "-o", str(OUT)]
+    BUILD.mkdir(exist_ok=True)
+    nvc = nvcc()
+    base = [nvc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+            "-Xcompiler", "-Wall", "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
     if verbose_ptxas:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [str(CSRC / s) for s in SOURCES]
-    cmd += ["-lcudart"]
-    print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+        base += ["-Xptxas", "-v"]
+    procs = []
+    for src, obj, extra in UNITS:
+        cmd = base + extra + ["-c", str(CSRC / src), "-o", str(BUILD / obj)]
+        print(" ".join(cmd), flush=True)
+        procs.append(subprocess.Popen(cmd))
+    bad = [u for u, p in zip(UNITS, procs) if p.wait() != 0]
+    if bad:
+        raise RuntimeError(f"nvcc failed on {[u[0] for u in bad]}")
+    link = [nvc, *ARCH, "-shared", "-o", str(OUT)] + [str(BUILD / u[1]) for u in UNITS]
+    link += ["-lcudart"]
+    print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
     return OUT
 
 

@@ -1262,6 +1262,20 @@ int mcs_lobes_alim(mcs_ctx* c, const mcs_modal* modals, size_t n_modals,
   return MCS_OK;
 }
 
+int mcs_measure_peaks(mcs_ctx* c, mcs_peaks* out) {
+  if (!c || !out) return fail(MCS_ERR_ARG, "NULL ctx or output");
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  DevBuf scratch;
+  int rc = scratch.ensure(16 << 10);
+  if (rc) return rc;
+  rc = measure_peaks(c->stream, c->sms, scratch.p, &out->fp32_tflops, &out->fp64_tflops,
+                     &out->smem_tbps);
+  cudaStreamSynchronize(c->stream);
+  scratch.release();
+  return rc;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------- allocation-free solve

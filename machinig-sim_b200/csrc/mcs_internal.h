@@ -123,18 +123,54 @@ struct KernelShape {
 // previous kernel of the stream (the previous bucket of a plan), which it may overlap once
 // all of that kernel's blocks are resident, and whose completion its own completion
 // implies.
-int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
-                 const PointParams* pts, const int32_t* order, int n, DevOpts opts,
-                 mcs_result* out, unsigned int* queue, const volatile int* cancel,
-                 unsigned int* progress, const GuideArgs& guide = GuideArgs(),
-                 int priority = 0, bool chained = false);
-int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
-                  const PointParams* pts, const TrialItem* items, int n, double chatter_idx,
-                  mcs_trial_result* out, unsigned int* queue, int priority = 0,
-                  bool chained = false);
-int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm);
-int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm);
-int set_smem_limits();
+// mcs_kernels.cu is built once per integration precision, into k32 and k64.
+#define MCS_KERNEL_API                                                                      \
+  int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,     \
+                   const PointParams* pts, const int32_t* order, int n, DevOpts opts,      \
+                   mcs_result* out, unsigned int* queue, const volatile int* cancel,       \
+                   unsigned int* progress, const GuideArgs& guide, int priority,           \
+                   bool chained);                                                          \
+  int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,    \
+                    const PointParams* pts, const TrialItem* items, int n,                 \
+                    double chatter_idx, mcs_trial_result* out, unsigned int* queue,        \
+                    int priority, bool chained);                                           \
+  int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm);            \
+  int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm);           \
+  int set_smem_limits();
+namespace k32 {
+MCS_KERNEL_API
+}
+namespace k64 {
+MCS_KERNEL_API
+}
+#undef MCS_KERNEL_API
+inline int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
+                        const PointParams* pts, const int32_t* order, int n, DevOpts opts,
+                        mcs_result* out, unsigned int* queue, const volatile int* cancel,
+                        unsigned int* progress, const GuideArgs& guide = GuideArgs(),
+                        int priority = 0, bool chained = false) {
+  return (shape.fp64 ? k64::launch_solve : k32::launch_solve)(
+      shape, grid, smem, stream, pts, order, n, opts, out, queue, cancel, progress, guide,
+      priority, chained);
+}
+inline int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t stream,
+                         const PointParams* pts, const TrialItem* items, int n,
+                         double chatter_idx, mcs_trial_result* out, unsigned int* queue,
+                         int priority = 0, bool chained = false) {
+  return (shape.fp64 ? k64::launch_trials : k32::launch_trials)(
+      shape, grid, smem, stream, pts, items, n, chatter_idx, out, queue, priority, chained);
+}
+inline int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm) {
+  return (shape.fp64 ? k64::occupancy_solve : k32::occupancy_solve)(shape, smem, blocks_per_sm);
+}
+inline int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm) {
+  return (shape.fp64 ? k64::occupancy_trials : k32::occupancy_trials)(shape, smem,
+                                                                      blocks_per_sm);
+}
+inline int set_smem_limits() {
+  const int rc = k32::set_smem_limits();
+  return rc ? rc : k64::set_smem_limits();
+}
 // surrogate (mcs_surrogate.cu)
 int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d_mu,
                              float* d_sigma, float2* d_guide, const mcs_guide_opts* g,
@@ -146,6 +182,9 @@ mcs_ctx* surrogate_ctx(mcs_surrogate* s);
 std::mutex& surrogate_mutex(mcs_surrogate* s);
 // guided plans that hold the surrogate (it cannot be destroyed while any do)
 void surrogate_hold(mcs_surrogate* s, int delta);
+// peak-rate probes (mcs_probe.cu); scratch: a device buffer of at least 16 KB
+int measure_peaks(cudaStream_t st, int sms, void* scratch, double* fp32_tflops,
+                  double* fp64_tflops, double* smem_tbps);
 int launch_lobes(cudaStream_t stream, const mcs_modal* modals, const mcs_lobe_query* qs, int n_q,
                  const double* rpm, int n_rpm, double* out);
 

@@ -36,12 +36,32 @@
 
 #include "mcs_internal.h"
 
+// The file is compiled once per integration precision (MCS_PREC = 32 or 64), into the
+// namespaces mcs::k32 and mcs::k64, so that the two halves of the template instances
+// build in parallel; mcs_internal.h dispatches on KernelShape::fp64.
+#ifndef MCS_PREC
+#define MCS_PREC 32
+#endif
+#if MCS_PREC == 64
+#define MCS_KNS k64
+#else
+#define MCS_KNS k32
+#endif
+
 namespace mcs {
+namespace MCS_KNS {
+#if MCS_PREC == 64
+using KScalar = double;
+#else
+using KScalar = float;
+#endif
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+#if MCS_PREC == 32
 constexpr float kLog2HRef = -4.321928094887363f;  // log2(H_REF = 0.05 mm), cutting.js:18
 constexpr float kHMin = 0.002f;                    // cutting.js:19
+#endif
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -52,6 +72,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Arithmetic of the integration scalar T (float or double).
 template <typename T>
 struct Arith;
+#if MCS_PREC == 32
 template <>
 struct Arith<float> {
   using V2 = float2;
@@ -68,6 +89,8 @@ struct Arith<float> {
   // correctly rounded float product
   static __device__ __forceinline__ float micro(float v) { return v * 1e6f; }
 };
+#endif
+#if MCS_PREC == 64
 template <>
 struct Arith<double> {
   using V2 = double2;
@@ -78,6 +101,7 @@ struct Arith<double> {
   static __device__ __forceinline__ double2 pair(double s, double c) { return make_double2(s, c); }
   static __device__ __forceinline__ float micro(double v) { return (float)(v * 1e6); }
 };
+#endif
 
 // Resident warps per SM the register allocation is held to (65536 / (32 * warps)); measured
 // on the sweep, any cap below the natural allocation spills and runs slower (1 = no cap).
@@ -89,11 +113,7 @@ struct Arith<double> {
 #endif
 template <typename T>
 struct MinWarps {
-  static constexpr int value = MCS_MIN_WARPS_F32;
-};
-template <>
-struct MinWarps<double> {
-  static constexpr int value = MCS_MIN_WARPS_F64;
+  static constexpr int value = MCS_PREC == 64 ? MCS_MIN_WARPS_F64 : MCS_MIN_WARPS_F32;
 };
 
 struct TrialOut {
@@ -903,13 +923,13 @@ void* trials_fn(bool nl) {
             : reinterpret_cast<void*>(&trials_kernel<T, SLOTS, NM, false>);
 }
 
+// The kernel of a shape in this file's precision (the caller dispatches on s.fp64).
 void* pick(bool solve, const KernelShape& s) {
+  if (s.fp64 != (MCS_PREC == 64 ? 1 : 0)) return nullptr;
 #define MCS_PICK(SL, NMV)                                                              \
   if (s.slots == SL && s.modes == NMV)                                                 \
-    return s.fp64 ? (solve ? solve_fn<double, SL, NMV>(s.nl, s.grouped)                 \
-                           : trials_fn<double, SL, NMV>(s.nl))                            \
-                  : (solve ? solve_fn<float, SL, NMV>(s.nl, s.grouped)                   \
-                           : trials_fn<float, SL, NMV>(s.nl));
+    return solve ? solve_fn<KScalar, SL, NMV>(s.nl, s.grouped)                         \
+                 : trials_fn<KScalar, SL, NMV>(s.nl);
   MCS_PICK(1, 1)
   MCS_PICK(1, 2)
   MCS_PICK(1, 3)
@@ -925,7 +945,7 @@ void* pick(bool solve, const KernelShape& s) {
 }  // namespace
 
 int set_smem_limits() {
-  for (int fp = 0; fp < 2; fp++)
+  const int fp = MCS_PREC == 64 ? 1 : 0;
   for (int nl = 0; nl < 2; nl++)
   for (int sl = 1; sl <= kMaxSlots; sl++)
     for (int nm = 1; nm <= kMaxModes; nm++)
@@ -993,4 +1013,5 @@ int launch_trials(const KernelShape& shape, int grid, int smem, cudaStream_t str
   return launch_with_priority(f, grid, smem, stream, args, priority, chained);
 }
 
+}  // namespace MCS_KNS
 }  // namespace mcs

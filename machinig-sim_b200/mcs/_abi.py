@@ -116,6 +116,11 @@ class PlanInfo(C.Structure):
                 ("n_points", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
 
+class Peaks(C.Structure):
+    _fields_ = [("fp32_tflops", C.c_double), ("fp64_tflops", C.c_double),
+                ("smem_tbps", C.c_double)]
+
+
 # numpy views of the record arrays (same layout as the ctypes structs)
 RESULT_DTYPE = np.dtype([("alim", "<f8"), ("lo", "<f8"), ("hi", "<f8"), ("open", "<i4"),
                          ("status", "<i4"), ("trials", "<i4"), ("steps_per_tooth", "<i4"),

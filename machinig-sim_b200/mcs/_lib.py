@@ -27,7 +27,7 @@ EXPORTS = (
     "mcs_default_train_opts", "mcs_default_guide_opts", "mcs_features", "mcs_surrogate_create",
     "mcs_surrogate_destroy", "mcs_surrogate_train", "mcs_surrogate_predict", "mcs_surrogate_grad",
     "mcs_surrogate_get_params", "mcs_surrogate_set_params", "mcs_solve_guided",
-    "mcs_plan_create_guided", "mcs_plan_guide_info", "mcs_tune",
+    "mcs_plan_create_guided", "mcs_plan_guide_info", "mcs_tune", "mcs_measure_peaks",
 )
 _VOID = ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free",
          "mcs_default_train_opts", "mcs_default_guide_opts")
@@ -97,6 +97,7 @@ def load(path: Path | str | None = None):
         L.mcs_solve_guided.argtypes = [vp, vp] + batch[1:] + [P(A.GuideOpts), vp, vp]
         L.mcs_plan_create_guided.argtypes = [vp, vp] + batch[1:] + [P(A.GuideOpts), P(vp)]
         L.mcs_plan_guide_info.argtypes = [vp, vp]
+        L.mcs_measure_peaks.argtypes = [vp, P(A.Peaks)]
         for name in EXPORTS:
             if name not in _VOID:
                 getattr(L, name).restype = C.c_int
@@ -306,6 +307,14 @@ class Context:
         check(self._L.mcs_lobes_alim(self._h, _ptr(m), len(m), C.cast(q, C.c_void_p),
                                      len(queries), _ptr(r), len(r), _ptr(out)))
         return out
+
+    def measure_peaks(self) -> dict:
+        """Measured FP32/FP64 FMA rates [TFLOP/s] and shared-memory bandwidth [TB/s] of this
+        device (mcs_measure_peaks): the solve kernels' roofline denominators."""
+        p = A.Peaks()
+        check(self._L.mcs_measure_peaks(self._h, C.byref(p)))
+        return {"fp32_tflops": p.fp32_tflops, "fp64_tflops": p.fp64_tflops,
+                "smem_tbps": p.smem_tbps}
 
     def close(self) -> None:
         if getattr(self, "_h", None):
