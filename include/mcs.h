@@ -122,7 +122,11 @@ typedef struct {
                               lane groups of one warp when their slice counts allow
                               (speculatively; only the trials on the decision path count);
                               1: one trial at a time.  Results are identical either way. */
-  int32_t pad;
+  int32_t coop_warps;      /* schedule: the heaviest points (up to one per SM) share their
+                              bisection among this many warps of one block, each running one
+                              trial of the next levels speculatively (2..8; 0: 8, narrowed to
+                              4 or 3 where 8 rings do not fit in shared memory; 1: off).
+                              Plain solves only.  Results are identical either way. */
 } mcs_opts;
 
 #define MCS_MAX_BUCKETS 32
@@ -175,7 +179,7 @@ typedef struct {
   int32_t modes;         /* modes per axis the kernel was built for */
   int32_t graph;         /* 1 when the launch is a captured CUDA graph */
   int32_t kernels;       /* kernel launches per execute */
-  int32_t pad;
+  int32_t coop_points;   /* points whose bisection several warps share (mcs_opts.coop_warps) */
   uint64_t n_points;
   uint64_t h2d_bytes; /* bytes a solve of these inputs copies host -> device */
   uint64_t d2h_bytes; /* bytes of results copied device -> host */

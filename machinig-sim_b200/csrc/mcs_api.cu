@@ -72,6 +72,8 @@ int check_inputs(const mcs_setup* setups, size_t n_setups, const mcs_modal* moda
     return fail(MCS_ERR_ARG, "max_buckets out of range [0, %d]", kMaxBuckets);
   if (o->serial_trials != 0 && o->serial_trials != 1)
     return fail(MCS_ERR_ARG, "serial_trials must be 0 or 1");
+  if (o->coop_warps < 0 || o->coop_warps > kCoopMaxWarpsHost)
+    return fail(MCS_ERR_ARG, "coop_warps out of range [0, %d]", kCoopMaxWarpsHost);
   for (size_t i = 0; i < n_setups; i++) {
     const mcs_setup& s = setups[i];
     const mcs_tool& t = s.tool;
@@ -381,11 +383,18 @@ namespace {
 
 // Orders the work items by cost (largest first) and groups them into buckets of similar
 // shared-memory need, each launched as its own persistent grid.
+//
+// Multi-warp bisection: the heaviest buckets of a plain solve, as long as their points
+// together number at most one per SM, run each point on `coop` warps of one block (the
+// latency tail of the slowest points; see solve_coop_kernel).  Buckets whose points pack
+// trials into lane groups keep them: that speculation needs no extra warps.  pp (NULL for
+// trial batches) gives the per-point sizes the multi-warp shared memory follows from.
 int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
                  const std::vector<int>& slots, const std::vector<int>& modes,
                  const std::vector<int>& nls, const std::vector<int>& grps, bool trials,
                  int fp64, int max_buckets,
-                 std::vector<int32_t>& order, std::vector<Bucket>& buckets) {
+                 std::vector<int32_t>& order, std::vector<Bucket>& buckets,
+                 const std::vector<PointParams>* pp = nullptr, int coop_warps = 1) {
   const int nbmax = max_buckets > 0 ? std::min(max_buckets, kMaxBuckets) : kDefaultBuckets;
   const size_t n = smem.size();
   std::vector<int32_t> idx(n);
@@ -427,6 +436,26 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     b.smem = (top + 15) & ~15;
     b.shape = KernelShape{sl, nm, fp64, nl, trials ? 0 : gr};
     order.insert(order.end(), seg.begin(), seg.end());
+    if (!trials && pp && coop_warps > 1 && gr == 0 && (int)order.size() <= ctx->sms) {
+      // the widest block whose rings fit: the requested width, else 4, else 3
+      for (int wv : {coop_warps, 4, 3}) {
+        if (wv > coop_warps) continue;
+        int cs = 0;
+        for (int32_t q : seg) {
+          const PointParams& P = (*pp)[q];
+          cs = std::max(cs, coop_smem(P.spr, fp64 != 0, P.ring_rows, P.lpad, wv));
+        }
+        cs = (cs + 15) & ~15;
+        if (cs > kCoopSmemLimit) continue;
+        KernelShape ks = b.shape;
+        ks.coop = wv;
+        int cb = 0;
+        if (occupancy_solve(ks, cs, &cb) != 0 || cb < 1) continue;
+        b.shape = ks;
+        b.smem = cs;
+        break;
+      }
+    }
     int bps = 0;
     const int rc = trials ? occupancy_trials(b.shape, b.smem, &bps)
                           : occupancy_solve(b.shape, b.smem, &bps);
@@ -624,9 +653,11 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
+  // multi-warp bisection for plain solves (0: 8 warps, narrowed where rings do not fit)
+  const int coop = sur ? 1 : (o->coop_warps == 0 ? kCoopMaxWarpsHost : o->coop_warps);
   rc = make_buckets(ctx, smem, cost, slots, modes, nls, grps, false, o->precision == MCS_FP64,
                     o->max_buckets, order,
-                    pl->buckets);
+                    pl->buckets, &pp, coop);
   if (rc) {
     discard(pl);
     return rc;
@@ -720,7 +751,7 @@ void mcs_default_opts(mcs_opts* o) {
   o->precision = MCS_FP32;
   o->max_buckets = 0;
   o->serial_trials = 0;
-  o->pad = 0;
+  o->coop_warps = 0;
 }
 
 const char* mcs_last_error(void) { return g_last_error.c_str(); }
@@ -822,8 +853,9 @@ int mcs_plan_info_get(const mcs_plan* pl, mcs_plan_info* info) {
   int warps = 0, smem = 0;
   for (const Bucket& b : pl->buckets) {
     info->blocks += b.grid;
-    warps = std::max(warps, b.blocks_per_sm);
+    warps = std::max(warps, b.blocks_per_sm * std::max(1, b.shape.coop));
     smem = std::max(smem, b.smem);
+    if (b.shape.coop > 0) info->coop_points += b.count;
   }
   info->warps_per_sm = warps;
   info->smem_per_warp = smem;

@@ -88,6 +88,17 @@ __host__ __device__ inline int warp_smem(int spr, bool fp64, int ring_rows, int 
   return extra_offset(spr, fp64, ring_rows, lpad) + groups * (kToothSamples * 8 + kTrialOutBytes);
 }
 
+// Multi-warp solve (several warps share one point's bisection, one trial per warp): the
+// table once, then a surface ring and a result record per warp.
+constexpr int kCoopMaxWarpsHost = 8;
+constexpr int kCoopSmemLimit = kMaxSmemPerWarp - 1024;  // dynamic bytes; static words beside
+__host__ __device__ inline int coop_ring_bytes(int ring_rows, int lpad) {
+  return (4 * ring_rows * lpad + 15) & ~15;
+}
+__host__ __device__ inline int coop_smem(int spr, bool fp64, int ring_rows, int lpad, int warps) {
+  return table_bytes(spr, fp64) + warps * (coop_ring_bytes(ring_rows, lpad) + kTrialOutBytes);
+}
+
 // Options the kernels read (mcs_opts reduced to what the device needs).
 struct DevOpts {
   double a_min, a_max, chatter_idx;
@@ -117,6 +128,7 @@ struct KernelShape {
   int fp64;   // 0: FP32 force law and modal integration, 1: FP64
   int nl;     // 1: size effect and/or process damping present
   int grouped = 0;  // 1: points may run several trials per warp in lane groups
+  int coop = 0;     // > 0: solve with this many warps per point (multi-warp bisection)
 };
 
 // Host launchers (mcs_kernels.cu).  chained = 1: a programmatic dependent launch behind the

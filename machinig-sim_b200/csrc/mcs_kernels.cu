@@ -868,6 +868,157 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
   chain_end();
 }
 
+// Speculative multi-warp bisection: the W = blockDim / 32 warps of a block share one
+// point's timeDomainLimit (stabtd.js:24-32).  A round runs the midpoints of the next
+// bisection levels, one trial per warp; the first round also runs the a_max probe beside
+// the first levels of [a_min, a_max].  A point's serial chain of iters + 1 trials becomes
+// about 1 + iters / log2(W + 1) rounds, which shortens the latency tail of the slowest
+// points on a GPU that has SMs to spare for them.  The midpoints are the same square roots
+// the serial bisection takes and only the trials on the decision path are counted, so the
+// results are those of one trial at a time.  Every warp runs the plain whole-warp trial
+// (the same code as the one-warp kernel) with its own surface ring; the sin/cos table is
+// shared.  All warps keep the same bracket state, decided from the round's results in
+// shared memory, and meet at block barriers, which every thread of the block reaches on
+// every round: the number of rounds is a function of that shared state.
+constexpr int kCoopMaxWarps = 8;
+static_assert(kCoopMaxWarps == kCoopMaxWarpsHost, "multi-warp block width");
+
+template <typename T, int SLOTS, int NM, bool NL>
+__global__ void __launch_bounds__(kCoopMaxWarps * kWarp) solve_coop_kernel(
+    const PointParams* __restrict__ pts, const int32_t* __restrict__ order, int n, DevOpts o,
+    mcs_result* __restrict__ out, unsigned int* __restrict__ queue, const volatile int* cancel,
+    unsigned int* progress) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned int s_item;
+  __shared__ int s_cancel;
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+  const int W = blockDim.x / kWarp;
+  // levels a round decides: the first beside the a_max probe (1 + 2^dtop - 1 <= W trials),
+  // the later ones alone (2^dbis - 1 <= W trials); W = 1 is the serial bisection
+  int dtop = 0, dbis = 1;
+  while ((2 << dtop) <= W) dtop++;
+  while ((2 << dbis) - 1 <= W) dbis++;
+  chain_start();
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
+    __syncthreads();
+    const unsigned int w = s_item;
+    if (w >= (unsigned)n) break;
+    const int pi = order[w];
+    const PointParams* P = pts + pi;
+    const bool fp64 = sizeof(T) == 8;
+    auto* table = reinterpret_cast<typename Arith<T>::V2*>(smem);
+    const int ring_bytes = coop_ring_bytes(P->ring_rows, P->lpad);
+    float* ring = reinterpret_cast<float*>(smem + table_bytes(P->spr, fp64) + warp * ring_bytes);
+    TrialOut* outs = reinterpret_cast<TrialOut*>(smem + table_bytes(P->spr, fp64) +
+                                                 W * ring_bytes);
+    mcs_result r;
+    r.status = MCS_OK;
+    r.trials = 0;
+    r.evals = 0;
+    r.engaged = 0;
+    r.steps_per_tooth = P->spt;
+    r.open = 0;
+    r.alim = r.lo = r.hi = 0.0;
+    // the cancel flag, read once per round by one thread so that every warp sees the same
+    auto cancelled = [&]() -> bool {
+      if (threadIdx.x == 0) s_cancel = (cancel != nullptr && *cancel != 0) ? 1 : 0;
+      __syncthreads();
+      const bool c = s_cancel != 0;
+      __syncthreads();
+      return c;
+    };
+    if (cancelled()) {
+      r.status = MCS_ERR_CANCELLED;
+    } else {
+      // the revolution's sin/cos table, built by the whole block
+      const double dphi = P->dphi;
+      for (int p = threadIdx.x; p < P->spr; p += blockDim.x) {
+        double sv, cv;
+        sincos(p * dphi, &sv, &cv);
+        table[p] = Arith<T>::pair(sv, cv);
+      }
+      __syncthreads();
+      auto account = [&](const TrialOut& t) -> bool {
+        r.trials++;
+        r.evals += t.evals;
+        r.engaged += t.engaged;
+        if (t.status != MCS_OK) r.status = t.status;
+        return t.index > o.chatter_idx;
+      };
+      double lo = o.a_min, hi = o.a_max;
+      int it = 0;
+      bool top = true;
+      for (;;) {
+        // ---- plan the round (identical in every thread) ----
+        double ap[kCoopMaxWarps];
+        int k0 = 0, lv;
+        if (top) {
+          ap[k0++] = o.a_max;
+          lv = min(dtop, o.iters);
+        } else {
+          if (it >= o.iters) {
+            r.alim = sqrt(lo * hi);
+            r.lo = lo;
+            r.hi = hi;
+            break;
+          }
+          if (cancelled()) {
+            r.status = MCS_ERR_CANCELLED;
+            r.alim = sqrt(lo * hi);
+            r.lo = lo;
+            r.hi = hi;
+            break;
+          }
+          lv = min(dbis, o.iters - it);
+        }
+        if (lv > 0) tree_midpoints(lo, hi, lv, ap + k0);
+        const int nt = k0 + (lv > 0 ? (1 << lv) - 1 : 0);
+        // ---- run: one trial per warp ----
+        if (warp < nt) {
+          Groups G;
+          one_group(G, ap[warp]);
+          simulate<T, SLOTS, NM, NL, false>(P, G, table, ring, nullptr, outs + warp, lane);
+        }
+        __syncthreads();
+        // ---- decide: the serial bisection's steps, in its order ----
+        bool done = false;
+        if (top) {
+          top = false;
+          if (!account(outs[0])) {
+            r.alim = o.a_max;
+            r.lo = o.a_max;
+            r.hi = INFINITY;
+            r.open = 1;
+            done = true;
+          }
+        }
+        if (!done) {
+          int node = 0;
+          for (int l = 0; l < lv; l++) {
+            const double mid = sqrt(lo * hi);
+            const bool c = account(outs[k0 + node]);
+            if (c)
+              hi = mid;
+            else
+              lo = mid;
+            it++;
+            node = 2 * node + (c ? 1 : 2);
+          }
+        }
+        __syncthreads();  // the round's results are read before the next round writes
+        if (done) break;
+      }
+    }
+    if (threadIdx.x == 0) {
+      out[pi] = r;
+      if (progress != nullptr) atomicAdd(progress, 1u);
+    }
+    __syncthreads();
+  }
+  chain_end();
+}
+
 // Batch of independent chatterAt trials (decision replay at given depths).
 template <typename T, int SLOTS, int NM, bool NL>
 __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) trials_kernel(const PointParams* __restrict__ pts,
@@ -918,6 +1069,11 @@ void* solve_fn(bool nl, bool gr) {
             : reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, false, false>);
 }
 template <typename T, int SLOTS, int NM>
+void* coop_fn(bool nl) {
+  return nl ? reinterpret_cast<void*>(&solve_coop_kernel<T, SLOTS, NM, true>)
+            : reinterpret_cast<void*>(&solve_coop_kernel<T, SLOTS, NM, false>);
+}
+template <typename T, int SLOTS, int NM>
 void* trials_fn(bool nl) {
   return nl ? reinterpret_cast<void*>(&trials_kernel<T, SLOTS, NM, true>)
             : reinterpret_cast<void*>(&trials_kernel<T, SLOTS, NM, false>);
@@ -928,8 +1084,9 @@ void* pick(bool solve, const KernelShape& s) {
   if (s.fp64 != (MCS_PREC == 64 ? 1 : 0)) return nullptr;
 #define MCS_PICK(SL, NMV)                                                              \
   if (s.slots == SL && s.modes == NMV)                                                 \
-    return solve ? solve_fn<KScalar, SL, NMV>(s.nl, s.grouped)                         \
-                 : trials_fn<KScalar, SL, NMV>(s.nl);
+    return !solve ? trials_fn<KScalar, SL, NMV>(s.nl)                                  \
+                  : s.coop > 0 ? coop_fn<KScalar, SL, NMV>(s.nl)                       \
+                               : solve_fn<KScalar, SL, NMV>(s.nl, s.grouped);
   MCS_PICK(1, 1)
   MCS_PICK(1, 2)
   MCS_PICK(1, 3)
@@ -949,10 +1106,12 @@ int set_smem_limits() {
   for (int nl = 0; nl < 2; nl++)
   for (int sl = 1; sl <= kMaxSlots; sl++)
     for (int nm = 1; nm <= kMaxModes; nm++)
-      for (int k = 0; k < 3; k++) {  // solve, grouped solve, trials
-        void* f = pick(k < 2, KernelShape{sl, nm, fp, nl, k == 1 ? 1 : 0});
-        cudaError_t e =
-            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerWarp);
+      for (int k = 0; k < 4; k++) {  // solve, grouped solve, trials, multi-warp solve
+        KernelShape ks{sl, nm, fp, nl, k == 1 ? 1 : 0};
+        if (k == 3) ks.coop = kCoopMaxWarps;
+        void* f = pick(k != 2, ks);
+        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             k == 3 ? kCoopSmemLimit : kMaxSmemPerWarp);
         if (e != cudaSuccess) return (int)e;
         e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return (int)e;
@@ -963,7 +1122,8 @@ int set_smem_limits() {
 int occupancy_solve(const KernelShape& shape, int smem, int* blocks_per_sm) {
   void* f = pick(true, shape);
   if (!f) return (int)cudaErrorInvalidValue;
-  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, kWarp, smem);
+  const int threads = kWarp * (shape.coop > 0 ? shape.coop : 1);
+  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, threads, smem);
 }
 
 int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm) {
@@ -972,15 +1132,16 @@ int occupancy_trials(const KernelShape& shape, int smem, int* blocks_per_sm) {
   return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, kWarp, smem);
 }
 
-// One-warp blocks with a scheduling priority (lower value = scheduled first).  A chained
+// Blocks of `warps` warps (one unless multi-warp) with a scheduling priority (lower value =
+// scheduled first).  A chained
 // launch is a programmatic dependent launch: it may start once every block of the
 // stream's previous kernel has started (chain_start), so the buckets of a plan take the
 // SMs in the order they are launched, longest points first.
 int launch_with_priority(void* f, int grid, int smem, cudaStream_t stream, void** args,
-                         int priority, bool chained) {
+                         int priority, bool chained, int warps = 1) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kWarp);
+  cfg.blockDim = dim3(kWarp * warps);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = stream;
   cudaLaunchAttribute attr[2];
@@ -999,6 +1160,12 @@ int launch_solve(const KernelShape& shape, int grid, int smem, cudaStream_t stre
                  unsigned int* progress, const GuideArgs& guide, int priority, bool chained) {
   void* f = pick(true, shape);
   if (!f) return (int)cudaErrorInvalidValue;
+  if (shape.coop > 0) {  // multi-warp bisection: plain points only
+    if (shape.coop > kCoopMaxWarps || guide.guide != nullptr || smem > kCoopSmemLimit)
+      return (int)cudaErrorInvalidValue;
+    void* args[] = {&pts, &order, &n, &opts, &out, &queue, &cancel, &progress};
+    return launch_with_priority(f, grid, smem, stream, args, priority, chained, shape.coop);
+  }
   GuideArgs g = guide;
   void* args[] = {&pts, &order, &n, &opts, &out, &queue, &cancel, &progress, &g};
   return launch_with_priority(f, grid, smem, stream, args, priority, chained);
