@@ -2,29 +2,38 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload ("sweep"): one milling setup -- 4 flutes, D 10 mm, helix 30 deg, 10 um runout,
-Ktc 700 / Krc 210 / Kte 20 / Kre 30, 3 modes per axis (fn 600-3000 Hz, k 5e6-5e7 N/m,
-zeta 0.01-0.05, seeded) -- swept over 4096 spindle speeds 3000-30000 rpm; each speed is a
-10-iteration geometric bisection over [0.05, 15] mm whose trials run 60 revolutions with
-40 slices and the reference's steps-per-tooth rule.  A step = the whole 4096-point sweep.
+Headline workload ("sweep", the plain method batched on the GPU): one milling setup -- 4
+flutes, D 10 mm, helix 30 deg, 10 um runout, Ktc 700 / Krc 210 / Kte 20 / Kre 30, 3 modes
+per axis (fn 600-3000 Hz, k 5e6-5e7 N/m, zeta 0.01-0.05, seeded) -- swept over 4096 spindle
+speeds 3000-30000 rpm; each speed is a 10-iteration geometric bisection over [0.05, 15] mm
+whose trials run 60 revolutions with 40 slices and the reference's steps-per-tooth rule.
+A step = the whole 4096-point sweep.
 
 `value`  points/s with the inputs resident on the device: the prepared batch is a
          captured CUDA graph (mcs_plan_execute), timed with CUDA events on the library's
          stream, L2 flushed (a 256 MiB write) between timed steps.
 `e2e`    the same through the public blocking call mcs_solve from page-locked host
          buffers: host preparation, H2D copies, the solve and the D2H of results per step.
-Multi-GPU (torchrun): every rank solves its own seeded 4096-point sweep (weak scaling, no
-collective on the data path); the time is the max over ranks.
+`accuracy`  the critical depths of the timed runs against the reference algorithm in FP64
+         on the host (the CPU restatement of stabtd.js/cutting.js) on the workload's seeded
+         256-point subset; that same host run is the `cpu_baseline` timing.
+`workloads.hetero`  the heterogeneous batch (16384 seeded setups, process damping and size
+         effect on, autotuned schedule, captured graph), measured the same way.
+`guided`  surrogate-guided serving of 65536 queries against the plain plan, repeated.
+Multi-GPU (torchrun): every rank solves its own seeded sweep (weak scaling, no collective
+on the data path); the time is the max over ranks.
 
 --impl reference: the reference's CPU path on the host cores.  The reference is
-JavaScript and no JS runtime exists on these machines, so this arm times the C++ FP64
-restatement of it (oracle/) with one thread per core on a bounded sample of the sweep.
+JavaScript and no JS runtime exists on these machines (probed and recorded in the line),
+so this arm times the C++ FP64 restatement of it (oracle/) with one thread per core on
+seeded, cost-sorted samples of the same workload, a fresh sample every step.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import shutil
 import subprocess
 import sys
 import threading
@@ -46,13 +55,14 @@ WORKLOADS = {
 }
 METRIC = "stability-boundary points/sec on 1 B200: surrogate-guided vs plain GPU vs Node CPU @<=2% depth err"
 UNIT = "points/s"
-FLOP_ENGAGED = 46.0   # FP32 flop per in-cut slice evaluation (force law, cutting.js:181-207)
+FLOP_ENGAGED = 46.0   # flop per in-cut slice evaluation (force law, cutting.js:181-207)
 FLOP_IDLE = 15.0      # per out-of-cut evaluation of the reference loop (angle, normal, store)
+SMEM_BYTES_ENGAGED = 8.0  # surface-ring load + store per in-cut evaluation (cutting.js:187-194)
 # DRAM bytes per point of one solve, from an ncu capture of a 3072-point sweep (FP32, 8
 # buckets): dram__bytes.sum.per_second x gpu__time_duration of each bucket launch, summed,
 # 4.63 MB per execution.  A point reads its parameters and writes its result once; the
 # trial state lives in registers and shared memory, so the bytes scale with the points.
-DRAM_BYTES_PER_POINT = {"sweep": 1508.0}
+DRAM_BYTES_PER_POINT = {("sweep", "fp32"): 1508.0}
 
 
 def env_rank():
@@ -132,41 +142,161 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def run_oracle_sample(wl, n_points: int, threads: int):
-    """FP64 oracle over the first n_points of a seeded permutation of the workload."""
+def node_probe() -> dict:
+    """Whether a JavaScript runtime exists here (the reference's own path needs one)."""
+    found = {n: shutil.which(n) for n in ("node", "nodejs", "deno", "bun")}
+    have = {k: v for k, v in found.items() if v}
+    rec = {"runtimes_found": have or None}
+    if not have:
+        rec["reference_js"] = ("unavailable on this box: no JavaScript runtime (node, nodejs, "
+                               "deno, bun) on PATH")
+    else:
+        rec["reference_js"] = ("unavailable on this box: a runtime exists but the reference's "
+                               "JavaScript sources are not on the GPU box")
+    return rec
+
+
+def point_cost(wl, idx) -> np.ndarray:
+    """Relative cost of each point (steps per trial x teeth x slices), for ordering host
+    work largest first: the reference step rule max(48, ceil(T_tooth f_top 24))."""
+    pts = wl.points[idx]
+    st = wl.setups[pts["setup"]]
+    md = wl.modals[pts["modal"]]
+    N = st["tool"]["N"].astype(np.float64)
+    fx = md["x"]["fn"].max(axis=1)
+    fy = np.where(md["ny"] > 0, md["y"]["fn"].max(axis=1), fx)
+    ftop = np.maximum(fx, fy)
+    S = np.maximum(100.0, pts["S"])
+    if wl.opts.steps_per_tooth:
+        spt = np.full(len(pts), float(wl.opts.steps_per_tooth))
+    else:
+        spt = np.maximum(48.0, np.ceil(60.0 / (S * N) * ftop * 24))
+    return spt * N * N
+
+
+def run_oracle(wl, idx, threads: int):
+    """The FP64 restatement of the reference over points idx (cost-sorted for the thread
+    pool); returns (results in idx order, seconds)."""
     import pyoracle as O
     from mcs import _abi as A
 
-    perm = np.argsort(np.random.default_rng(7).random(wl.n))[:n_points]
+    idx = np.asarray(idx)
+    order = np.argsort(-point_cost(wl, idx), kind="stable")
     setups = [A.Setup.from_buffer_copy(r.tobytes()) for r in wl.setups]
     modals = [A.Modal.from_buffer_copy(r.tobytes()) for r in wl.modals]
-    pts = wl.points[np.sort(perm)]
+    pts = wl.points[idx[order]]
     P = (A.Point * len(pts)).from_buffer_copy(pts.tobytes())
     t = time.perf_counter()
-    O.solve_batch(setups, modals, P, wl.opts, nthreads=threads)
-    return len(pts), time.perf_counter() - t
+    res, _ = O.solve_batch(setups, modals, P, wl.opts, nthreads=threads)
+    dt = time.perf_counter() - t
+    out = np.empty_like(res)
+    out[order] = res
+    return out, dt
 
 
-def cpu_baseline(wl, target_s: float = 15.0) -> dict:
+def fp64_subset(wl) -> np.ndarray:
+    """The workload's seeded 256-point subset (the golden fixtures hold the same points)."""
+    from mcs import workloads as W
+
+    if "fp64_subset" in wl.meta:
+        return np.asarray(wl.meta["fp64_subset"])
+    return np.sort(np.argsort(W.uniform(np.arange(wl.n), 7, 0))[:256])
+
+
+def within(a, b, tol=0.02) -> float:
+    both_open = (a["open"] == 1) & (b["open"] == 1)
+    rel = np.where(both_open, 0.0, np.abs(a["alim"] / b["alim"] - 1))
+    return float(np.mean(rel <= tol))
+
+
+def cpu_leg(wl) -> tuple[dict, np.ndarray, np.ndarray]:
+    """cpu_baseline: the FP64 restatement on all host cores over the seeded 256-point
+    subset; its results are also the accuracy reference of the GPU runs."""
     cores = cpu_cores()
-    n = min(wl.n, max(16, 2 * cores))
-    npts, dt = run_oracle_sample(wl, n, cores)
-    if dt < target_s / 3 and npts < wl.n:  # too short to be a stable figure: grow once
-        n2 = min(wl.n, int(npts * target_s / max(dt, 1e-3) * 0.5))
-        if n2 > npts:
-            npts, dt = run_oracle_sample(wl, n2, cores)
-    return {"value": npts / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{npts} of the {wl.n} {wl.name} points (seeded), C++ FP64 restatement of "
-                      f"stabtd.js/cutting.js, {cores} threads on {cpu_model()}"}
+    idx = fp64_subset(wl)
+    res, dt = run_oracle(wl, idx, cores)
+    rec = {"value": len(idx) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"the seeded {len(idx)}-point subset of the {wl.n} {wl.name} points "
+                     f"(cost-sorted), C++ FP64 restatement of stabtd.js/cutting.js, {cores} "
+                     f"threads on {cpu_model()}, {dt:.1f} s"}
+    return rec, idx, res
 
 
-def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool) -> dict:
+def pinned(torch, arr):
+    t = torch.empty(max(1, arr.nbytes), dtype=torch.uint8, pin_memory=True)
+    v = t.numpy()[: arr.nbytes].view(arr.dtype)
+    v[:] = arr
+    return t, v
+
+
+def e2e_leg(ctx, torch, wl, opts, info, steps, warmup, maxover, barrier, pts_total, ref):
+    """Points/s through the public blocking call mcs_solve from page-locked host buffers."""
+    import ctypes as C
+
+    import mcs
+    from mcs import _abi as A
+
+    hs = [pinned(torch, wl.setups), pinned(torch, wl.modals), pinned(torch, wl.points)]
+    out_t = torch.empty(len(wl.points) * A.RESULT_DTYPE.itemsize, dtype=torch.uint8,
+                        pin_memory=True)
+    out_v = out_t.numpy().view(A.RESULT_DTYPE)
+    L = ctx._L
+    args_c = (ctx._h, C.c_void_p(hs[0][1].ctypes.data), len(wl.setups),
+              C.c_void_p(hs[1][1].ctypes.data), len(wl.modals),
+              C.c_void_p(hs[2][1].ctypes.data), len(wl.points), C.byref(opts),
+              C.c_void_p(out_v.ctypes.data))
+    for _ in range(max(1, warmup)):
+        mcs._lib.check(L.mcs_solve(*args_c))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        mcs._lib.check(L.mcs_solve(*args_c))
+    torch.cuda.synchronize()
+    e2e_s = maxover(time.perf_counter() - t0) / steps
+    barrier()
+    assert out_v.tobytes() == ref.tobytes(), "e2e and plan results differ"
+    return {"value": pts_total / e2e_s, "unit": UNIT, "steps": steps,
+            "h2d_bytes_per_step": int(info["h2d_bytes"]),
+            "d2h_bytes_per_step": int(info["d2h_bytes"])}
+
+
+def roofline(res, step_ms, precision, peaks, clocks, workload, n_points) -> dict:
+    """The solve kernel's work against the measured FMA-issue peak of its precision."""
+    evals = float(res["evals"].sum())
+    engaged = float(res["engaged"].sum())
+    flop = FLOP_ENGAGED * engaged + FLOP_IDLE * (evals - engaged)
+    t = float(np.mean(step_ms)) / 1e3
+    achieved = flop / t / 1e12
+    key = "fp32_tflops" if precision == "fp32" else "fp64_tflops"
+    peak = peaks[key]
+    smem = SMEM_BYTES_ENGAGED * engaged / t / 1e12
+    traffic = DRAM_BYTES_PER_POINT.get((workload, precision))
+    return {"bound": precision, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "traffic": traffic * n_points if traffic else None,
+            "traffic_unit": "DRAM bytes per step, scaled by points from an ncu capture of a "
+                            "3072-point FP32 sweep" if traffic else None,
+            "peak_source": f"measured on this GPU (mcs_measure_peaks: {precision.upper()} FMA "
+                           f"issue, every SM occupied, CUDA events), of measured",
+            "smem": {"achieved_tbps": smem, "peak_tbps": peaks["smem_tbps"],
+                     "frac": smem / peaks["smem_tbps"],
+                     "note": "algorithmic surface-ring bytes: 8 B per in-cut evaluation"},
+            "work": f"{FLOP_ENGAGED:.0f} flop per in-cut and {FLOP_IDLE:.0f} per out-of-cut "
+                    f"reference evaluation; {evals:.3e} evaluations, {engaged:.3e} in cut "
+                    f"per step",
+            "clock_mhz": clocks["sm_mhz"]}
+
+
+def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool, repeats: int) -> dict:
     """Surrogate-guided serving: 65536 seeded hetero queries (30 % of the setups outside the
     training seeds), the trained model's guided plan against the plain plan on the same
-    queries, with agreement against the plain GPU bisection and, on a seeded 512-query
-    subset, against the FP64 restatement of the reference on the host."""
+    queries, each timed over `repeats` executions (median and spread), with agreement
+    against the plain GPU bisection and, on a seeded 512-query subset, against the FP64
+    restatement of the reference on the host."""
     from mcs import _abi as A
     from mcs import surrogate as SG
+    from mcs import tune as T
     from mcs import workloads as W
 
     if not SG.DEFAULT_MODEL.exists():
@@ -177,50 +307,53 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool) -> dict:
 
     def run(plan):
         plan.execute()  # warm-up (graph upload)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        with torch.cuda.stream(stream):
-            flush.fill_(7)
-        a.record(stream)
         plan.execute()
-        b.record(stream)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b), plan.results()
-
-    from mcs import tune as T
+        times = []
+        for i in range(repeats):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+            a.record(stream)
+            plan.execute()
+            b.record(stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        return times, plan.results()
 
     sv.opts.max_buckets, tuned = T.autotune(ctx, sv.setups, sv.modals, sv.points, sv.opts,
                                             device_name=torch.cuda.get_device_name(device))
     with ClockSampler(device) as clk:
         pp = ctx.plan(sv.setups, sv.modals, sv.points, sv.opts)
-        plain_ms, plain = run(pp)
+        plain_t, plain = run(pp)
         pp.close()
         gp = ctx.plan(sv.setups, sv.modals, sv.points, sv.opts, surrogate=sur)
-        guided_ms, gres = run(gp)
+        guided_t, gres = run(gp)
         info = gp.guide_info()
         gp.close()
     sur.close()
+    plain_ms, guided_ms = float(np.median(plain_t)), float(np.median(guided_t))
     path = info["path"]
     both_open = (gres["open"] == 1) & (plain["open"] == 1)
     rel = np.where(both_open, 0.0, np.abs(gres["alim"] / plain["alim"] - 1))
     out = np.asarray(sv.meta["outside"])
     sub = np.asarray(sv.meta["fp64_subset"])
-    # FP64 references on the subset: the GPU FP64 bisection and the host FP64 restatement
     o64 = A.make_opts(precision="fp64")
     for f in ("a_min", "a_max", "iters", "revs", "nonlinear", "honor_runout", "steps_per_tooth",
               "slices", "chatter_idx"):
         setattr(o64, f, getattr(sv.opts, f))
     g64 = ctx.solve(sv.setups, sv.modals, sv.points[sub], o64)
-
-    def within(a, b):
-        op = (a["open"] == 1) & (b["open"] == 1)
-        return float(np.mean(op | (np.abs(a["alim"] / b["alim"] - 1) <= 0.02)))
-
+    ratios = np.array(plain_t) / np.array(guided_t)
     res = {
         "workload": f"serve: {sv.n} seeded hetero (setup, speed) queries, "
                     f"{float(out.mean()):.0%} outside the training seeds",
         "value": sv.n / (guided_ms / 1e3), "unit": UNIT,
-        "plain_value": sv.n / (plain_ms / 1e3), "speedup_vs_plain": plain_ms / guided_ms,
+        "plain_value": sv.n / (plain_ms / 1e3),
+        "speedup_vs_plain": plain_ms / guided_ms,
+        "repeats": repeats,
+        "plain_ms": {"median": plain_ms, "min": min(plain_t), "max": max(plain_t)},
+        "guided_ms": {"median": guided_ms, "min": min(guided_t), "max": max(guided_t)},
+        "speedup_spread": [float(ratios.min()), float(ratios.max())],
         "trials_ratio": float(gres["trials"].sum() / plain["trials"].sum()),
         "paths": {A.PATH_NAMES[k]: float(np.mean(path == k)) for k in range(4)},
         "fallback_rate": float(np.mean(path == A.PATH_FALLBACK)),
@@ -251,21 +384,53 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool) -> dict:
     return res
 
 
+def make_workload(name: str, rank: int, points: int = 0):
+    from mcs import workloads as W
+
+    if name == "hetero":  # 16384 seeded setups per rank (weak scaling)
+        wl = W.hetero(n=16384, first_seed=16384 * rank)
+    else:
+        wl = W.sweep(seed=1 + rank)
+    if points and points < wl.n:  # a smaller case of the same workload (profiling)
+        wl = wl.subset(np.linspace(0, wl.n - 1, points).round().astype(int))
+    return wl
+
+
+def workload_config(name: str, wl) -> dict:
+    """The workload a line measures; identical in both arms."""
+    return {"workload": WORKLOADS[name], "points_per_gpu": int(wl.n)}
+
+
 def reference_arm(args) -> int:
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    from mcs import workloads as W
-
-    wl = W.hetero(n=16384) if args.workload == "hetero" else W.sweep()
+    wl = make_workload(args.workload, 0, args.points)
     cores = cpu_cores()
-    n = min(wl.n, max(8, cores))
-    for _ in range(args.warmup):
-        run_oracle_sample(wl, n, cores)
+    # seeded sample order over the whole workload; every step takes the next slice, so the
+    # steps together cover the speed range instead of repeating one fixed sample
+    perm = np.argsort(np.random.default_rng(7).random(wl.n))
+    pos = 0
+
+    def take(n):
+        nonlocal pos
+        idx = perm[np.arange(pos, pos + n) % wl.n]
+        pos += n
+        return idx
+
+    # calibration (the first warm-up step): per-step sample sized so that the whole run
+    # stays within a few minutes, and at least 8 points per thread (the pool's tail)
+    steps_total = args.steps + args.warmup
+    per_step_s = min(8.0, max(2.0, 150.0 / steps_total))
+    _, dt0 = run_oracle(wl, take(2 * cores), cores)
+    rate0 = 2 * cores / dt0
+    n_step = int(min(wl.n, max(8 * cores, round(rate0 * per_step_s / cores) * cores)))
+    for _ in range(args.warmup - 1):
+        run_oracle(wl, take(n_step), cores)
     tot_p, tot_t = 0, 0.0
     for _ in range(args.steps):
-        p, t = run_oracle_sample(wl, n, cores)
-        tot_p += p
+        _, t = run_oracle(wl, take(n_step), cores)
+        tot_p += n_step
         tot_t += t
     v = tot_p / tot_t
     line = {
@@ -273,12 +438,13 @@ def reference_arm(args) -> int:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOADS[args.workload],
-                   "sample_points_per_step": n},
+        "config": workload_config(args.workload, wl),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{n} seeded {wl.name} points per step; the reference is "
-                                   f"JavaScript with no JS runtime on this box, so its C++ "
-                                   f"FP64 restatement runs, {cores} threads, {cpu_model()}"},
+                         "sample": f"{n_step} seeded {wl.name} points per step (a fresh slice "
+                                   f"of a seeded permutation each step, cost-sorted), the C++ "
+                                   f"FP64 restatement of stabtd.js/cutting.js, {cores} "
+                                   f"threads, {cpu_model()}"},
+        "node_probe": node_probe(),
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -299,20 +465,13 @@ def ours(args) -> int:
     device = local if torch.cuda.is_available() else 0
     torch.cuda.set_device(device)
     import mcs
+    from mcs import _abi as A
     from mcs import tune as T
-    from mcs import workloads as W
 
-    if args.workload == "hetero":  # 16384 seeded setups per rank (weak scaling)
-        wl = W.hetero(n=16384, first_seed=16384 * rank)
-    else:
-        wl = W.sweep(seed=1 + rank)
-    if args.points and args.points < wl.n:  # a smaller case of the same workload (profiling)
-        wl = wl.subset(np.linspace(0, wl.n - 1, args.points).round().astype(int))
-    if args.serial_trials:
-        wl.opts.serial_trials = 1
     ctx = mcs.Context(device)
     stream = torch.cuda.ExternalStream(ctx.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    peaks = ctx.measure_peaks()  # roofline denominators, before any timed region
 
     def barrier():
         if dist is not None:
@@ -325,12 +484,16 @@ def ours(args) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed(precision: str):
-        """Device-resident plan of the sweep: per-step CUDA-event times, results, info."""
+    def timed(wl, precision: str, steps: int, warmup: int):
+        """Device-resident plan of a workload: per-step CUDA-event times, results, info."""
         opts = A.make_opts(precision=precision)
         for f in ("a_min", "a_max", "iters", "revs", "nonlinear", "honor_runout",
-                  "steps_per_tooth", "slices", "chatter_idx", "serial_trials"):
+                  "steps_per_tooth", "slices", "chatter_idx", "serial_trials", "coop_warps"):
             setattr(opts, f, getattr(wl.opts, f))
+        if args.serial_trials:
+            opts.serial_trials = 1
+        if args.coop_warps >= 0:
+            opts.coop_warps = args.coop_warps
         # schedule (number of shared-memory size classes) from the autotuner, untimed
         if args.max_buckets:
             opts.max_buckets, tuned = args.max_buckets, {"ms": {}, "cached": False}
@@ -340,17 +503,19 @@ def ours(args) -> int:
         plan = ctx.plan(wl.setups, wl.modals, wl.points, opts)
         info = plan.info()
         info["schedule"] = {"max_buckets": int(opts.max_buckets), "tuning_ms": tuned["ms"],
-                            "from_cache": bool(tuned["cached"])}
-        for _ in range(args.warmup):
+                            "from_cache": bool(tuned["cached"]),
+                            "coop_warps": int(opts.coop_warps),
+                            "coop_points": int(info["coop_points"])}
+        for _ in range(warmup):
             plan.execute()
         res = plan.results()
         assert np.all((res["status"] == 0) | (res["status"] == 4)), np.unique(res["status"])
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         barrier()
         torch.cuda.synchronize()
         with ClockSampler(device) as clk:
-            for i in range(args.steps):
+            for i in range(steps):
                 with torch.cuda.stream(stream):
                     flush.fill_(i & 0xFF)  # write 256 MiB (> 126 MB L2) between timed steps
                 starts[i].record(stream)
@@ -359,113 +524,96 @@ def ours(args) -> int:
             torch.cuda.synchronize()
         barrier()
         step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
-        res = plan.results()
+        res2 = plan.results()
+        assert res2.tobytes() == res.tobytes(), "results changed between executions"
         plan.close()
-        return step_ms, res, info, clk.summary(), opts
+        ms = maxover(float(np.sum(step_ms))) / steps
+        return {"step_ms": step_ms, "ms": ms, "res": res, "info": info,
+                "clocks": clk.summary(), "opts": opts}
 
-    from mcs import _abi as A
+    def measure(name: str, precisions, steps: int, warmup: int, e2e_steps: int, cpu: bool):
+        """One workload: every precision timed as a plan, the headline precision also end
+        to end; on rank 0 of a 1-GPU run the host FP64 baseline and the accuracy."""
+        wl = make_workload(name, rank, args.points)
+        pts_total = wl.n * world
+        var = {p: timed(wl, p, steps, warmup) for p in precisions}
+        head = var[precisions[0]]
+        e2e = None
+        if e2e_steps:
+            e2e = e2e_leg(ctx, torch, wl, head["opts"], head["info"], e2e_steps,
+                          max(1, warmup // 2), maxover, barrier, pts_total, head["res"])
+        rec = {"wl": wl, "var": var, "e2e": e2e, "pts_total": pts_total, "cpu": None,
+               "accuracy": None}
+        if cpu and rank == 0 and world == 1:
+            cpu_rec, idx, r64 = cpu_leg(wl)
+            rec["cpu"] = cpu_rec
+            rec["accuracy"] = {
+                "reference": "FP64 restatement of the reference on the host, seeded "
+                             f"{len(idx)}-point subset",
+                **{f"within_2pct_of_cpu_fp64_{p}": within(v["res"][idx], r64)
+                   for p, v in var.items()}}
+        return rec
 
-    variants = {}
-    for prec in (["fp32", "fp64"] if not args.fp32_only else [args.precision]):
-        step_ms, res, info, clocks, opts = timed(prec)
-        ms = maxover(float(np.sum(step_ms))) / args.steps
-        variants[prec] = {"step_ms": step_ms, "ms": ms, "res": res, "info": info,
-                          "clocks": clocks, "opts": opts}
-    main = variants[args.precision]
-    step_ms, ms, res, info, clocks = (main["step_ms"], main["ms"], main["res"], main["info"],
-                                      main["clocks"])
-    pts_total = wl.n * world
-    value = pts_total / (ms / 1e3)
+    def summarize(name: str, rec: dict, precision: str) -> dict:
+        v = rec["var"][precision]
+        return {
+            "value": rec["pts_total"] / (v["ms"] / 1e3), "unit": UNIT, "ms_per_step": v["ms"],
+            "config": workload_config(name, rec["wl"]),
+            "roofline": roofline(v["res"], v["step_ms"], precision, peaks, v["clocks"], name,
+                                 rec["wl"].n),
+            "e2e": rec["e2e"], "cpu_baseline": rec["cpu"], "accuracy": rec["accuracy"],
+            "launch": {"variant": f"plain GPU bisection, {precision} force law and modal "
+                                  "integration, FP64 statistics and bracket",
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "kernels_per_step": v["info"]["kernels"],
+                       "graph": bool(v["info"]["graph"]), "blocks": v["info"]["blocks"],
+                       "smem_per_warp_max": v["info"]["smem_per_warp"],
+                       "schedule": v["info"]["schedule"]},
+            "variants": {p: {"value": rec["pts_total"] / (x["ms"] / 1e3),
+                             "ms_per_step": x["ms"], "kernels_per_step": x["info"]["kernels"],
+                             "sm_mhz": x["clocks"]["sm_mhz"],
+                             "roofline_frac": roofline(x["res"], x["step_ms"], p, peaks,
+                                                       x["clocks"], name, rec["wl"].n)["frac"]}
+                         for p, x in rec["var"].items()},
+            "clocks": v["clocks"],
+        }
 
-    # algorithmic work of one step (same inputs every step): the reference loop's
-    # evaluations, in cut and out of cut
-    evals = float(res["evals"].sum())
-    engaged = float(res["engaged"].sum())
-    flop = FLOP_ENGAGED * engaged + FLOP_IDLE * (evals - engaged)
-    achieved_tflops = flop / (float(np.mean(step_ms)) / 1e3) / 1e12
-    sms = torch.cuda.get_device_properties(device).multi_processor_count
-    f_mhz = clocks["sm_mhz"] or 1965.0
-    peak_tflops = sms * 128 * 2 * f_mhz * 1e6 / 1e12
+    precs = [args.precision] + ([] if args.headline_only else
+                                [p for p in ("fp64", "fp32") if p != args.precision])
+    main = measure(args.workload, precs, args.steps, args.warmup,
+                   0 if args.no_e2e else max(2, min(args.steps, 5)), not args.no_cpu)
+    hetero = None
+    if not args.no_hetero and args.workload != "hetero":
+        hetero = measure("hetero", precs, max(3, min(args.steps, 5)), 3,
+                         0 if args.no_e2e else 2, not args.no_cpu)
 
-    # ---- e2e: public blocking API from page-locked host buffers ----
-    e2e = None
-    def pinned(arr):
-        t = torch.empty(arr.nbytes, dtype=torch.uint8, pin_memory=True)
-        v = t.numpy().view(arr.dtype)
-        v[:] = arr
-        return t, v
-
-    if not args.no_e2e:
-        keep = []
-        hs = [pinned(wl.setups), pinned(wl.modals), pinned(wl.points)]
-        keep += hs
-        out_t = torch.empty(len(wl.points) * A.RESULT_DTYPE.itemsize, dtype=torch.uint8,
-                            pin_memory=True)
-        out_v = out_t.numpy().view(A.RESULT_DTYPE)
-        import ctypes as C
-
-        L = ctx._L
-        args_c = (ctx._h, C.c_void_p(hs[0][1].ctypes.data), len(wl.setups),
-                  C.c_void_p(hs[1][1].ctypes.data), len(wl.modals),
-                  C.c_void_p(hs[2][1].ctypes.data), len(wl.points), C.byref(main["opts"]),
-                  C.c_void_p(out_v.ctypes.data))
-        for _ in range(max(1, args.warmup // 2)):
-            mcs._lib.check(L.mcs_solve(*args_c))
-        e2e_steps = max(2, min(args.steps, 5))
-        barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            mcs._lib.check(L.mcs_solve(*args_c))
-        torch.cuda.synchronize()
-        e2e_s = maxover(time.perf_counter() - t0) / e2e_steps
-        barrier()
-        assert np.array_equal(out_v["alim"], res["alim"]), "e2e and plan results differ"
-        e2e = {"value": pts_total / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(info["h2d_bytes"]),
-               "d2h_bytes_per_step": int(info["d2h_bytes"])}
-
-    line = None
     if rank == 0:
-        cpu = cpu_baseline(wl) if world == 1 and not args.no_cpu else None
-        guided = (guided_serve(ctx, torch, stream, flush, device, args.no_cpu)
+        head = summarize(args.workload, main, args.precision)
+        v = main["var"][args.precision]
+        guided = (guided_serve(ctx, torch, stream, flush, device, args.no_cpu,
+                               args.guided_repeats)
                   if world == 1 and not args.no_guided else None)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32" else "f64",
-            "data": "synthetic (seeded sweep; no public dataset exists for this path)",
-            "config": {"workload": WORKLOADS[args.workload],
-                       "points_per_gpu": wl.n,
-                       "variant": f"plain GPU bisection, {args.precision} force law and "
-                                  "modal integration, FP64 statistics and bracket",
-                       "l2": "flushed between timed steps (256 MiB write)",
-                       "kernels_per_step": info["kernels"], "graph": bool(info["graph"]),
-                       "blocks": info["blocks"], "smem_per_warp_max": info["smem_per_warp"],
-                       "schedule": info["schedule"]},
-            "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops,
-                         "unit": "TFLOP/s", "frac": achieved_tflops / peak_tflops,
-                         "traffic": (DRAM_BYTES_PER_POINT[args.workload] * wl.n
-                                     if args.workload in DRAM_BYTES_PER_POINT
-                                     and args.precision == "fp32" else None),
-                         "traffic_unit": "bytes per step, scaled by points from an ncu "
-                                         "capture of a 3072-point FP32 sweep",
-                         "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 flop x "
-                                        f"{f_mhz:.0f} MHz sampled SM clock (no FP32 figure "
-                                        "in MEASURED_PEAKS.json)",
-                         "work": f"{FLOP_ENGAGED:.0f} flop per in-cut and {FLOP_IDLE:.0f} per "
-                                 f"out-of-cut reference evaluation; {evals:.3e} evaluations, "
-                                 f"{engaged:.3e} in cut per step"},
-            "cpu_baseline": cpu,
+            "data": "synthetic (seeded; no public dataset exists for this path)",
+            "config": head["config"],
+            "launch": head["launch"],
+            "roofline": head["roofline"],
+            "cpu_baseline": head["cpu_baseline"],
+            "accuracy": head["accuracy"],
+            "e2e": head["e2e"],
+            "gpu_launches": int(v["info"]["kernels"]) * args.steps,
+            "clocks": head["clocks"],
+            "peaks": peaks,
+            "results": {"open": int(v["res"]["open"].sum()),
+                        "alim_median": float(np.median(v["res"]["alim"]))},
+            "variants": head["variants"],
+            "workloads": {"hetero": summarize("hetero", hetero, args.precision)}
+            if hetero else None,
             "guided": guided,
-            "e2e": e2e,
-            "gpu_launches": int(info["kernels"]) * args.steps,
-            "clocks": clocks,
-            "results": {"open": int(res["open"].sum()), "alim_median": float(np.median(res["alim"]))},
-            "variants": {k: {"value": pts_total / (v["ms"] / 1e3), "ms_per_step": v["ms"],
-                             "kernels_per_step": v["info"]["kernels"],
-                             "sm_mhz": v["clocks"]["sm_mhz"]} for k, v in variants.items()},
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -482,18 +630,23 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
-                    help="integration precision of the headline value")
-    ap.add_argument("--fp32-only", action="store_true", help="time only the headline precision")
+    ap.add_argument("--precision", default="fp64", choices=["fp32", "fp64"],
+                    help="integration precision of the headline value (the other is a variant)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="time only the headline precision")
     ap.add_argument("--points", type=int, default=0,
                     help="solve an evenly spaced subset of the workload (profiling case)")
-    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end legs")
     ap.add_argument("--no-guided", action="store_true",
                     help="skip the surrogate-guided serving leg")
+    ap.add_argument("--no-hetero", action="store_true", help="skip the hetero workload leg")
+    ap.add_argument("--guided-repeats", type=int, default=5)
     ap.add_argument("--workload", default="sweep", choices=["sweep", "hetero"],
                     help="sweep (the headline) or the heterogeneous batch")
     ap.add_argument("--max-buckets", type=int, default=0,
                     help="fixed schedule (shared-memory size classes); 0: autotune")
+    ap.add_argument("--coop-warps", type=int, default=-1,
+                    help="warps sharing each heaviest point's bisection (1: off; -1: default)")
     ap.add_argument("--serial-trials", action="store_true",
                     help="one bisection trial per warp at a time (same results)")
     a = ap.parse_args(argv)
