@@ -88,6 +88,8 @@ struct Arith<float> {
   // product of a float and 1e6 is exact in double, so rounding it to float gives the
   // correctly rounded float product
   static __device__ __forceinline__ float micro(float v) { return v * 1e6f; }
+  // a product the compiler may not fuse into a neighbouring addition
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
 };
 #endif
 #if MCS_PREC == 64
@@ -100,6 +102,7 @@ struct Arith<double> {
   }
   static __device__ __forceinline__ double2 pair(double s, double c) { return make_double2(s, c); }
   static __device__ __forceinline__ float micro(double v) { return (float)(v * 1e6); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 };
 #endif
 
@@ -249,12 +252,16 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
     len[s] = 0;
     base[s] = (gb + k) * lpad;
     if (k < nz && !P->empty) {
-      const double b = fmin(dz, ap - k * dz);
-      const double zr = k * dz + 0.5 * b;
+      // separately rounded products and sums, as the reference evaluates them: a product
+      // left to the compiler may or may not be fused into the addition next to it, and two
+      // kernels that inline this code could then disagree in the last bit
+      const double kdz = __dmul_rn((double)k, dz);
+      const double b = fmin(dz, __dsub_rn(ap, kdz));
+      const double zr = __dadd_rn(kdz, __dmul_rn(0.5, b));
       double r = P->R, kap = 1.0;
       if (P->type == MCS_TOOL_BALL && zr < P->R) {
         const double d = P->R - zr;
-        r = sqrt(fmax(1e-6, P->R * P->R - d * d));
+        r = sqrt(fmax(1e-6, __dsub_rn(__dmul_rn(P->R, P->R), __dmul_rn(d, d))));
         kap = r / P->R;
       }
       const double lag = zr * P->tanB / P->R;
@@ -377,7 +384,7 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
         float* cell = ring + base[s] + j;
         const float* src = act[s] ? cell : reinterpret_cast<const float*>(table);
         const T prev = (T)*src;
-        const T feedH = fzk[s] * sn;
+        const T feedH = A::mul(fzk[s], sn);  // not fused into the sums below
         T h = (feedH + rn) - prev;
         const bool cut = h > T(0);
         // out of cut the old surface survives one more feed step (cutting.js:193)
@@ -493,7 +500,7 @@ __device__ void simulate(const PointParams* __restrict__ P, const Groups& G,
       const double tx = mine ? (double)ts.x : 0.0, ty = mine ? (double)ts.y : 0.0;
       const double mx = warp_sum(tx) / n, my = warp_sum(ty) / n;
       const double ex = mine ? (double)ts.x - mx : 0.0, ey = mine ? (double)ts.y - my : 0.0;
-      const double vv = warp_sum(ex * ex + ey * ey);
+      const double vv = warp_sum(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)));
       const double once = sqrt(vv / n) * 1e6;
       const double md = P->hist_m ? (double)P->hist_m : 1.0;
       double w = (sxx - sx * sx / md) + (syy - sy * sy / md);
