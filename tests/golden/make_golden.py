@@ -9,6 +9,8 @@ Writes, per workload, the oracle's timeDomainLimit results and the full trial tr
   sweep.npz    the 256-speed FP64 subset of the 4096-speed sweep
   hetero.npz   256 seeded setups of the heterogeneous batch
   edge.npz     edge cases: slot / up milling / ball end / 1 and 8 flutes / > 32 slices
+  self_agreement.npz  the reference's own sweep and hetero limits under 1e-6 / 1e-5 feed
+               changes (how well it agrees with itself)
 
 The oracle is a restatement of the reference (src/stabtd.js, src/cutting.js) pinned by the
 reference's own known answers (tests/test_oracle_pins.py); these files freeze its output
@@ -104,6 +106,40 @@ def sensitivity(wl, pts, res, tr, threads, eps):
     return dmax, flip
 
 
+# relative feed changes of the self-agreement fixture: the FP64 reference's own limits
+# under an input change of the size an FP32 trajectory's rounding amounts to
+SELF_LEVELS = [1e-6, -1e-6, 1e-5]
+
+
+def self_agreement(out: Path, threads: int):
+    """self_agreement.npz: for the sweep and hetero subsets, the FP64 reference's
+    timeDomainLimit with the feed scaled by (1 + eps) for each eps of SELF_LEVELS.  Where a
+    1e-6 change of an input moves the reference's own limit by more than 2 %, no
+    integration in another precision can be expected to land within 2 % of it either; the
+    GPU parity tests compare their FP32 agreement with this one."""
+    rec = {"levels": np.array(SELF_LEVELS)}
+    for name, wl, idx in (("sweep", W.sweep(), np.array(W.sweep().meta["fp64_subset"])),
+                          ("hetero", W.hetero(),
+                           np.sort(np.argsort(W.uniform(np.arange(16384), 7, 0))[:256]))):
+        wl = compact(wl, idx)
+        modals = [A.Modal.from_buffer_copy(r.tobytes()) for r in wl.modals]
+        P = (A.Point * len(wl.points)).from_buffer_copy(wl.points.tobytes())
+        alim, opn = [], []
+        t = time.time()
+        for eps in SELF_LEVELS:
+            st = wl.setups.copy()
+            st["fz"] *= 1 + eps
+            setups = [A.Setup.from_buffer_copy(r.tobytes()) for r in st]
+            res, _ = O.solve_batch(setups, modals, P, wl.opts, nthreads=threads)
+            alim.append(res["alim"])
+            opn.append(res["open"])
+        rec[f"{name}_alim"] = np.stack(alim)
+        rec[f"{name}_open"] = np.stack(opn)
+        print(f"{out.name}: {name} {len(idx)} points x {len(SELF_LEVELS)} feeds in "
+              f"{time.time() - t:.1f} s", flush=True)
+    np.savez_compressed(out, **rec)
+
+
 def edge_workload() -> W.Workload:
     """Cases off the benchmark grid: slot, up milling, ball end, N = 1 and 8, 48 slices,
     helix 0 (every slice in phase), a multi-mode asymmetric tool and an empty arc."""
@@ -163,7 +199,7 @@ def main(argv=None):
     ap.add_argument("--only", default="")
     a = ap.parse_args(argv)
     th = a.threads or O.cpu_count()
-    todo = a.only.split(",") if a.only else ["small", "edge", "sweep", "hetero"]
+    todo = a.only.split(",") if a.only else ["small", "edge", "sweep", "hetero", "self"]
     if "small" in todo:
         w = W.small()
         run(w, np.arange(w.n), th, HERE / "small.npz")
@@ -177,6 +213,8 @@ def main(argv=None):
         w = W.hetero()
         idx = np.sort(np.argsort(W.uniform(np.arange(w.n), 7, 0))[:256])
         run(w, idx, th, HERE / "hetero.npz")
+    if "self" in todo:
+        self_agreement(HERE / "self_agreement.npz", th)
     return 0
 
 

@@ -43,3 +43,44 @@ def test_fixtures_cover_their_workloads():
         g = load_golden(name)
         assert g["sens_flip"].shape == (len(g["sens_levels"]),) + g["traces"].shape
         assert g["sens_levels"][0] == 1e-7
+
+
+def _within(alim, ref_alim, opn, ref_open, tol=0.02):
+    both = (opn == 1) & (ref_open == 1)
+    rel = np.where(both, 0.0, np.abs(alim / ref_alim - 1))
+    return rel <= tol
+
+
+def test_self_agreement_fixture_reproduces(oracle):
+    """self_agreement.npz is the oracle's timeDomainLimit under scaled feeds: recomputing
+    two of its points gives the same bits."""
+    from mcs import _abi as A
+
+    s = load_golden("self_agreement")
+    g = load_golden("sweep")
+    idx = [0, 117]
+    setups = g["setups"].copy()
+    setups["fz"] *= 1 + s["levels"][0]
+    S = [A.Setup.from_buffer_copy(r.tobytes()) for r in setups]
+    M = [A.Modal.from_buffer_copy(r.tobytes()) for r in g["modals"]]
+    pts = g["points"][idx]
+    P = (A.Point * len(pts)).from_buffer_copy(pts.tobytes())
+    res, _ = oracle.solve_batch(S, M, P, A.opts_from_record(g["opts"]), nthreads=0)
+    assert res["alim"].tobytes() == s["sweep_alim"][0][idx].tobytes()
+
+
+@pytest.mark.parametrize("name", ["sweep", "hetero"])
+def test_reference_disagrees_with_itself_under_a_1e6_feed_change(name):
+    """The FP64 reference's own critical depths are ill-conditioned near chaotic chatter:
+    scaling the feed by 1 +- 1e-6 (about what the rounding of an FP32 trajectory amounts
+    to) moves more than 1 % of the limits by more than 2 %.  This is why FP32 integration
+    cannot meet a 2 %-on-99 % bar against FP64 on these workloads, and why the parity tests
+    hold FP32 to the reference's own agreement under that change."""
+    s = load_golden("self_agreement")
+    g = load_golden(name)
+    ref = g["results"]
+    for k, eps in enumerate(s["levels"]):
+        ok = _within(s[f"{name}_alim"][k], ref["alim"], s[f"{name}_open"][k], ref["open"])
+        print(f"{name}: feed x (1 + {eps:g}): {ok.sum()}/{len(ok)} within 2 % of the reference")
+        if abs(eps) == 1e-6:
+            assert ok.mean() < 0.99
