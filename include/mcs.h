@@ -375,6 +375,43 @@ int mcs_plan_create_guided(mcs_ctx* ctx, mcs_surrogate* s, const mcs_setup* setu
                            const mcs_guide_opts* g, mcs_plan** plan);
 int mcs_plan_guide_info(mcs_plan* plan, mcs_guide_info* info);
 
+/* ------------------------------------------------------------------ spindle speed model
+ * Tool-tip modes that change with spindle speed: modesAt of src/spindle.js:64-85, which the
+ * Simulator's modalNow(S) applies (src/sim.js:229-233) to give every point of a lobe sweep
+ * its own modal set (src/main.js:495-496).  Host arithmetic, FP64; no device needed.
+ *  - measured FRFs at several speeds (cfg.modal.speedFrfs) replace the model: the modes are
+ *    interpolated linearly between the measurements (by mode order when the counts match,
+ *    else the nearer measurement's), held constant outside the measured range;
+ *  - else, with two_dof, the tool on a spindle mode: two tip modes of a two-mass model whose
+ *    spindle spring softens with speed (spindle.js:38-53, 75-78);
+ *  - else the rest modes scaled through the compliance chain 1/k = 1/k_tool + 1/k_s(S):
+ *    k' = k f, fn' = fn sqrt(f), with the bearing softening k_s(S) = k_s0 / (1 + c (S/S_ref)^2),
+ *    c = drop / (1 - drop) (spindle.js:18-30, 55, 79-84).
+ */
+typedef struct {
+  double S;         /* spindle speed of the measurement [rpm] */
+  mcs_modal modes;  /* tool-tip modes measured at S (ny == 0: y takes the x modes) */
+} mcs_speed_frf;
+
+typedef struct {
+  mcs_modal rest;       /* modes at rest (modal.modesX/modesY, or the one {k, fn, zeta}) */
+  double drop;          /* bearing-stiffness loss at s_ref, clamped to [0, 0.9]
+                           (spindle.js SOFT_DEFAULT: 0.25) */
+  double s_ref;         /* [rpm]; 0 reads as 30000 */
+  double k_tool, k_sp;  /* compliance chain [N/mm]: tool bending, spindle/holder; a value
+                           <= 0 means no chain (the rest modes at every speed) */
+  int32_t two_dof;      /* 1: two tip modes from the tool (k_tool, m_tool, z_tool) on the
+                           spindle mode (k_sp, m_sp, z_sp) */
+  int32_t pad;
+  double m_tool, m_sp;  /* [kg] */
+  double z_tool, z_sp;  /* damping ratios */
+} mcs_spindle;
+
+/* The modal set at each speed S[i] into out[i] (n_frfs = 0: the model without
+ * measurements).  Output sets always give ny explicitly. */
+int mcs_modes_at(const mcs_spindle* spindle, const mcs_speed_frf* frfs, size_t n_frfs,
+                 const double* S, size_t n_speeds, mcs_modal* out);
+
 /* ------------------------------------------------------------------ measurement
  * Peak rates of the context's device, measured with CUDA events on its stream: FP32 and
  * FP64 FMA issue (2 flop per FMA, every SM fully occupied) and shared-memory bandwidth

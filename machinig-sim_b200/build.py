@@ -18,7 +18,8 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libmcs.so"
-SOURCES = ["mcs_kernels.cu", "mcs_lobes.cu", "mcs_surrogate.cu", "mcs_probe.cu", "mcs_api.cu"]
+SOURCES = ["mcs_kernels.cu", "mcs_lobes.cu", "mcs_surrogate.cu", "mcs_probe.cu", "mcs_spindle.cpp",
+           "mcs_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -36,6 +37,7 @@ UNITS = [("mcs_kernels.cu", "mcs_kernels_f32.o", ["-DMCS_PREC=32"]),
          ("mcs_lobes.cu", "mcs_lobes.o", []),
          ("mcs_surrogate.cu", "mcs_surrogate.o", []),
          ("mcs_probe.cu", "mcs_probe.o", []),
+         ("mcs_spindle.cpp", "mcs_spindle.o", []),
          ("mcs_api.cu", "mcs_api.o", [])]
 
 

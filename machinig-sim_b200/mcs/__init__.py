@@ -6,6 +6,7 @@ The functions mirror the reference's JavaScript API for this path:
   timeDomainLimits (the Worker sweep) src/stabworker.js:6-14
   StabWorker (the message protocol)   src/stabworker.js:1-15
   lobeLimit (stabilityLobes + alimAt) src/sld.js:23-76
+  spindle.Spindle (modesAt)           src/spindle.js:64-85, sim.modalNow (sim.js:229-233)
 
 Surrogate (an MLP trained on the solver's own limits) guides the bisection of
 Context.solve_guided and guided plans; mcs.surrogate trains and stores one.
@@ -17,11 +18,13 @@ from ._abi import (CHATTER_IDX, DEFAULTS, make_material, make_modal, make_opts, 
 from ._lib import (Context, Job, MCSError, Plan, Surrogate, default_context,
                    default_guide_opts, default_train_opts, load)
 from .sld import lobeLimit, lobeLimits
+from .spindle import Spindle, lobe_speeds, sweep_points, tool_model
 from .stabtd import chatterAt, chatterIndex, timeDomainLimit, timeDomainLimits
 from .worker import StabWorker
 
 __all__ = [
-    "CHATTER_IDX", "DEFAULTS", "Context", "Job", "MCSError", "Plan", "StabWorker", "Surrogate",
+    "CHATTER_IDX", "DEFAULTS", "Context", "Job", "MCSError", "Plan", "Spindle", "StabWorker",
+    "Surrogate", "lobe_speeds", "sweep_points", "tool_model",
     "chatterAt", "chatterIndex", "default_context", "default_guide_opts",
     "default_train_opts", "load", "lobeLimit", "lobeLimits",
     "make_material", "make_modal", "make_opts", "make_setup", "make_tool", "timeDomainLimit",

@@ -116,6 +116,17 @@ class PlanInfo(C.Structure):
                 ("n_points", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
 
+class SpeedFrf(C.Structure):
+    _fields_ = [("S", C.c_double), ("modes", Modal)]
+
+
+class Spindle(C.Structure):
+    _fields_ = [("rest", Modal), ("drop", C.c_double), ("s_ref", C.c_double),
+                ("k_tool", C.c_double), ("k_sp", C.c_double), ("two_dof", C.c_int32),
+                ("pad", C.c_int32), ("m_tool", C.c_double), ("m_sp", C.c_double),
+                ("z_tool", C.c_double), ("z_sp", C.c_double)]
+
+
 class Peaks(C.Structure):
     _fields_ = [("fp32_tflops", C.c_double), ("fp64_tflops", C.c_double),
                 ("smem_tbps", C.c_double)]

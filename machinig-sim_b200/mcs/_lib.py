@@ -28,6 +28,7 @@ EXPORTS = (
     "mcs_surrogate_destroy", "mcs_surrogate_train", "mcs_surrogate_predict", "mcs_surrogate_grad",
     "mcs_surrogate_get_params", "mcs_surrogate_set_params", "mcs_solve_guided",
     "mcs_plan_create_guided", "mcs_plan_guide_info", "mcs_tune", "mcs_measure_peaks",
+    "mcs_modes_at",
 )
 _VOID = ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free",
          "mcs_default_train_opts", "mcs_default_guide_opts")
@@ -98,6 +99,7 @@ def load(path: Path | str | None = None):
         L.mcs_plan_create_guided.argtypes = [vp, vp] + batch[1:] + [P(A.GuideOpts), P(vp)]
         L.mcs_plan_guide_info.argtypes = [vp, vp]
         L.mcs_measure_peaks.argtypes = [vp, P(A.Peaks)]
+        L.mcs_modes_at.argtypes = [P(A.Spindle), vp, C.c_size_t, vp, C.c_size_t, vp]
         for name in EXPORTS:
             if name not in _VOID:
                 getattr(L, name).restype = C.c_int

@@ -61,11 +61,20 @@ def timeDomainLimit(tool, modal, mat, S, arc, fz, opts: Mapping[str, Any] | None
 
 
 def timeDomainLimits(tool, mat, arc, fz, points: Sequence[Mapping[str, Any]],
-                     opts: Mapping[str, Any] | None = None, *, ctx: Context | None = None):
+                     opts: Mapping[str, Any] | None = None, *, ctx: Context | None = None,
+                     spindle=None):
     """The Worker's sweep in one call: points = [{S, modal}] (stabworker.js:8-13).
+    With a spindle model (mcs.spindle.Spindle) a point may leave out its modal: it gets
+    the modes at its own speed, as sim.modalNow(S) gives them (main.js:495-496).
     Returns [{S, alim, open}] in point order."""
     setups = [A.make_setup(tool, mat, arc, fz)]
-    modals = [A.make_modal(p["modal"]) for p in points]
+    need = [i for i, p in enumerate(points) if p.get("modal") is None]
+    if need and spindle is None:
+        raise ValueError("points without a modal need a spindle model")
+    at = spindle.modes_at([float(points[i]["S"]) for i in need]) if need else []
+    own = dict(zip(need, at))
+    modals = [A.Modal.from_buffer_copy(own[i].tobytes()) if i in own
+              else A.make_modal(p["modal"]) for i, p in enumerate(points)]
     pts = A.points_array(np.zeros(len(points)), np.arange(len(points)),
                          [float(p["S"]) for p in points])
     res = _ctx(ctx).solve(setups, modals, pts, A.make_opts(opts))

@@ -10,6 +10,7 @@ setup is a pure function of its seed and any subset can be regenerated on its ow
   hetero      16384 seeded setups, process damping and size effect on
   train       262144 (setup, speed) points for surrogate labels, 90/10 split by seed
   serve       65536 queries, 30 % from seeds outside the training range
+  spindle     the Worker's 18-speed lobe curve with each speed's own modes (spindle.js)
 
 Fixed choices the benchmark leaves open: flute length 25 mm (the Simulator default,
 src/sim.js:45); Kac = Kae = 0 (they act only on Fz); Kre = Kte * U(1.1, 1.5) and
@@ -239,6 +240,64 @@ def serve(n: int = 65536, train_setups: int = 16384, outside: float = 0.3) -> Wo
     perm = np.argsort(uniform(q, 6, 3))
     return Workload("serve", st, md, pts, A.make_opts(HETERO_OPTS),
                     {"queries": n, "outside": out, "fp64_subset": np.sort(perm[:512]).tolist()})
+
+
+# Speed-dependent modes (src/spindle.js): the cases of the reference's spindle tests
+# (test/spindle.test.mjs:47-49, 82-88, 98-103) on the Simulator's defaults (sim.js:44-46):
+# a 3-flute D10 tool with a short stickout on a 50 kN/mm spindle that loses 25 % bearing
+# stiffness at 30000 rpm; the same tool with a spindle/holder mode; and FRFs measured at
+# 0 and 30000 rpm, interpolated between.
+SPINDLE_CASES = {
+    "chain": {"tool": {"D": 10.0, "stickout": 15.0, "kSpindle": 50000.0},
+              "modal": {"auto": True, "k": 0.0, "fn": 0.0, "zeta": 0.04}},
+    "spindle_mode": {"tool": {"D": 10.0, "stickout": 15.0, "kSpindle": 50000.0},
+                     "modal": {"auto": True, "k": 0.0, "fn": 0.0, "zeta": 0.04},
+                     "spindle_mode": {"on": True, "fn": 1200.0, "zeta": 0.05}},
+    "measured": {"tool": {"D": 10.0, "stickout": 30.0, "kSpindle": 50000.0},
+                 "modal": {"k": 10000.0, "fn": 3000.0, "zeta": 0.03, "speedFrfs": [
+                     {"S": 0.0, "modesX": [{"k": 12000.0, "fn": 3000.0, "zeta": 0.03}]},
+                     {"S": 30000.0, "modesX": [{"k": 9000.0, "fn": 2400.0, "zeta": 0.04}]}]}},
+}
+
+
+def spindle_sweep(speeds=None) -> Workload:
+    """The Worker's lobe curve with speed-dependent modes (main.js:494-501): for each case
+    of SPINDLE_CASES the 18 log-spaced speeds over 4000-30000 rpm, each point with the modal
+    set sim.modalNow(S) gives (mcs.spindle); half-immersion down milling with the
+    Simulator's A5052 (materials.js:25), fz 0.05 mm, 3 flutes, helix 30, flute length 12 mm
+    (the 7.4 kHz tool mode of the two-mass case needs 888 steps per tooth at 4000 rpm, and
+    a slot's surface window would not fit in shared memory); the reference's
+    timeDomainLimit options ([0.05, 20] x 8, 120 revolutions, size effect and process
+    damping)."""
+    from . import spindle as SP
+
+    speeds = SP.lobe_speeds() if speeds is None else list(speeds)
+    names = list(SPINDLE_CASES)
+    st = np.zeros(len(names), dtype=A.SETUP_DTYPE)
+    st["tool"]["N"] = 3
+    st["tool"]["type"] = A.TOOL_FLAT
+    st["tool"]["R"] = 5.0
+    st["tool"]["helix_deg"] = 30.0
+    st["tool"]["flute_len"] = 12.0
+    st["mat"]["Ktc"], st["mat"]["Krc"] = 700.0, 210.0
+    st["mat"]["Kte"], st["mat"]["Kre"] = 20.0, 25.0
+    st["mat"]["mc"], st["mat"]["Ci"] = 0.10, 2e4
+    st["arc_st"], st["arc_ex"] = math.pi / 2, math.pi
+    st["fz"] = 0.05
+    modals, pts = [], []
+    for c, name in enumerate(names):
+        case = SPINDLE_CASES[name]
+        sp = SP.Spindle.from_tool(case["tool"], case["modal"],
+                                  spindle_mode=case.get("spindle_mode"))
+        for j, r in enumerate(sp.modes_at(speeds)):
+            pts.append((c, len(modals), speeds[j]))
+            modals.append(r)
+    points = np.zeros(len(pts), dtype=A.POINT_DTYPE)
+    points["setup"] = [p[0] for p in pts]
+    points["modal"] = [p[1] for p in pts]
+    points["S"] = [p[2] for p in pts]
+    return Workload("spindle", st, np.array(modals, dtype=A.MODAL_DTYPE), points,
+                    A.make_opts(), {"cases": names, "speeds": speeds})
 
 
 CONFIGS = {"small": small, "sweep": sweep, "hetero": hetero, "train": train, "serve": serve}

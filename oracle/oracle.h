@@ -135,6 +135,9 @@ double or_sdm_limit(const or_sdm_params* p, double a_max);
 /* ---- tool.js / identify.js ---- */
 /* toolModel of a uniform beam: out = {k [N/mm], fn [Hz], kTool [N/mm], mEff [kg]}. */
 void or_tool_model(double D, double stickout, double k_spindle, double m_holder, double out[4]);
+// spindle.js modesAt at each speed (spindle.cpp)
+void or_modes_at(const mcs_spindle* sp, const mcs_speed_frf* frfs, size_t n_frfs,
+                 const double* S, size_t n, mcs_modal* out);
 /* immersion(mode, ae, D): mode 0 slot, 1 down, 2 up; out = {phiSt, phiEx}. */
 void or_immersion(int mode, double ae, double D, double out[2]);
 

@@ -109,6 +109,9 @@ def lib():
     L.or_sdm_limit.restype = C.c_double
     L.or_tool_model.argtypes = [C.c_double] * 4 + [P(C.c_double)]
     L.or_immersion.argtypes = [C.c_int, C.c_double, C.c_double, P(C.c_double)]
+    L.or_modes_at.argtypes = [P(A.Spindle), C.c_void_p, C.c_size_t, P(C.c_double), C.c_size_t,
+                              C.c_void_p]
+    L.or_modes_at.restype = None
     _LIB = L
     return L
 
@@ -334,3 +337,14 @@ def cpu_count() -> int:
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- spindle.js
+def modes_at(spindle: A.Spindle, speeds, frfs=()) -> np.ndarray:
+    """modesAt (src/spindle.js:64-85) at each speed: MODAL_DTYPE records."""
+    S = np.ascontiguousarray(speeds, dtype=np.float64)
+    F = A.array_of(A.SpeedFrf, list(frfs))
+    out = np.zeros(max(1, len(S)), dtype=A.MODAL_DTYPE)
+    lib().or_modes_at(C.byref(spindle), C.cast(F, C.c_void_p), len(frfs), _dptr(S), len(S),
+                      C.c_void_p(out.ctypes.data))
+    return out[: len(S)]

@@ -11,6 +11,7 @@ Writes, per workload, the oracle's timeDomainLimit results and the full trial tr
   edge.npz     edge cases: slot / up milling / ball end / 1 and 8 flutes / > 32 slices
   self_agreement.npz  the reference's own sweep and hetero limits under 1e-6 / 1e-5 feed
                changes (how well it agrees with itself)
+  spindle.npz  the 18-speed lobe curve with speed-dependent modes (spindle.js), 3 cases
 
 The oracle is a restatement of the reference (src/stabtd.js, src/cutting.js) pinned by the
 reference's own known answers (tests/test_oracle_pins.py); these files freeze its output
@@ -140,6 +141,24 @@ def self_agreement(out: Path, threads: int):
     np.savez_compressed(out, **rec)
 
 
+def spindle_workload() -> W.Workload:
+    """The speed-dependent sweep of mcs.workloads.spindle_sweep with every modal set from
+    the oracle's own restatement of modesAt (src/spindle.js:64-85), not the library's."""
+    from mcs import spindle as SP
+
+    wl = W.spindle_sweep()
+    speeds = wl.meta["speeds"]
+    modals = []
+    for name in wl.meta["cases"]:
+        case = W.SPINDLE_CASES[name]
+        sp = SP.Spindle.from_tool(case["tool"], case["modal"],
+                                  spindle_mode=case.get("spindle_mode"))
+        frfs = A.array_of(A.SpeedFrf, sp.frfs)
+        modals.append(O.modes_at(sp.record, speeds, list(frfs)[: len(sp.frfs)]))
+    wl.modals = np.concatenate(modals)
+    return wl
+
+
 def edge_workload() -> W.Workload:
     """Cases off the benchmark grid: slot, up milling, ball end, N = 1 and 8, 48 slices,
     helix 0 (every slice in phase), a multi-mode asymmetric tool and an empty arc."""
@@ -199,7 +218,8 @@ def main(argv=None):
     ap.add_argument("--only", default="")
     a = ap.parse_args(argv)
     th = a.threads or O.cpu_count()
-    todo = a.only.split(",") if a.only else ["small", "edge", "sweep", "hetero", "self"]
+    todo = (a.only.split(",") if a.only else
+            ["small", "edge", "sweep", "hetero", "self", "spindle"])
     if "small" in todo:
         w = W.small()
         run(w, np.arange(w.n), th, HERE / "small.npz")
@@ -215,6 +235,9 @@ def main(argv=None):
         run(w, idx, th, HERE / "hetero.npz")
     if "self" in todo:
         self_agreement(HERE / "self_agreement.npz", th)
+    if "spindle" in todo:
+        w = spindle_workload()
+        run(w, np.arange(w.n), th, HERE / "spindle.npz")
     return 0
 
 

@@ -36,7 +36,7 @@ DEPTH_QUANTILE = {"fp64": 0.98, "fp32": 0.95}
 MIN_AGREE = {"fp64": 0.99, "fp32": 0.97}
 INDEX_RTOL = 2e-3
 INDEX_ATOL = 1e-4
-FIXTURES = ["small", "edge", "sweep", "hetero"]
+FIXTURES = ["small", "edge", "sweep", "hetero", "spindle"]
 PRECISIONS = ["fp32", "fp64"]
 
 
