@@ -435,6 +435,30 @@ int mcs_lobes_alim(mcs_ctx* ctx, const mcs_modal* modals, size_t n_modals,
                    const mcs_lobe_query* queries, size_t n_queries, const double* rpm,
                    size_t n_rpm, double* alim);
 
+/*
+ * The speed-dependent lobe diagram of the chart (Simulator.lobes, src/sim.js:262-287, with
+ * LOBE_NODE and LOBE_STEP of sim.js:37): for speed-dependent dynamics the reference builds
+ * one zero-order diagram per MCS_LOBE_NODE rpm over [0.8 rpm_min, 1.1 rpm_max), each with
+ * the modal set at its node's centre (modesAt, see mcs_modes_at) and read (alimAt) every
+ * MCS_LOBE_STEP rpm across its own node only, into one composite curve; uncovered speeds
+ * read 1e3.  The chart then reads that curve per pixel (charts.js:170-185), which
+ * mcs_curve_alim does.  base gives N, lobes, Ktc, Krc, the arc and the speed range (its
+ * modal index is ignored).  *n_out receives the curve's length; with rpm == NULL nothing
+ * else happens (a size query), else cap must hold it.  The per-node diagrams run on the
+ * GPU, one CTA each.
+ */
+#define MCS_LOBE_NODE 1000
+#define MCS_LOBE_STEP 25
+int mcs_lobes_composite(mcs_ctx* ctx, const mcs_spindle* spindle, const mcs_speed_frf* frfs,
+                        size_t n_frfs, const mcs_lobe_query* base, double* rpm, double* alim,
+                        size_t cap, size_t* n_out);
+/* alimAt (sld.js:64-76) of one lobe polyline of n_curve points at each of n speeds: the
+ * interpolation on the consecutive pairs a, b with a.rpm <= S <= b.rpm, the minimum where
+ * several cover S, +inf where none does.  Host arithmetic (a binary search when the speeds
+ * ascend, as they do in stabilityLobes' lobes and the composite curve). */
+int mcs_curve_alim(const double* curve_rpm, const double* curve_alim, size_t n_curve,
+                   const double* rpm, size_t n, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1294,6 +1294,118 @@ int mcs_lobes_alim(mcs_ctx* c, const mcs_modal* modals, size_t n_modals,
   return MCS_OK;
 }
 
+int mcs_lobes_composite(mcs_ctx* c, const mcs_spindle* sp, const mcs_speed_frf* frfs,
+                        size_t n_frfs, const mcs_lobe_query* base, double* rpm_out,
+                        double* alim_out, size_t cap, size_t* n_out) {
+  if (!c || !sp || !base || !n_out) return fail(MCS_ERR_ARG, "NULL ctx, spindle, base or n_out");
+  const mcs_lobe_query& B = *base;
+  if (B.N < 1 || B.lobes < 0 || B.lobes > 10000 ||
+      !(is_finite(B.Ktc) && B.Ktc != 0 && is_finite(B.Krc) && is_finite(B.phi_st) &&
+        is_finite(B.phi_ex) && is_finite(B.rpm_min) && is_finite(B.rpm_max)))
+    return fail(MCS_ERR_ARG, "base lobe query is invalid");
+  // the nodes and their speeds, as Simulator.lobes walks them (sim.js:275-281)
+  const double lo = B.rpm_min * 0.8, hi = B.rpm_max * 1.1;
+  if ((hi - lo) / MCS_LOBE_NODE > 100000)
+    return fail(MCS_ERR_ARG, "speed range of %g rpm is too wide", hi - lo);
+  std::vector<double> centre, samples;
+  std::vector<mcs_lobe_query> qs;
+  std::vector<int> begin, count;
+  for (double S0 = lo; S0 < hi; S0 += MCS_LOBE_NODE) {
+    mcs_lobe_query q = B;
+    q.rpm_min = S0;
+    q.rpm_max = S0 + MCS_LOBE_NODE;
+    q.modal = (uint32_t)qs.size();
+    qs.push_back(q);
+    centre.push_back(S0 + MCS_LOBE_NODE / 2);
+    begin.push_back((int)samples.size());
+    for (double S = S0; S < std::min(hi, S0 + MCS_LOBE_NODE); S += MCS_LOBE_STEP)
+      samples.push_back(S);
+    count.push_back((int)samples.size() - begin.back());
+  }
+  *n_out = samples.size();
+  if (!rpm_out) return MCS_OK;
+  if (!alim_out) return fail(MCS_ERR_ARG, "alim is NULL");
+  if (cap < samples.size())
+    return fail(MCS_ERR_ARG, "the curve has %zu points, cap is %zu", samples.size(), cap);
+  std::vector<mcs_modal> modals(qs.size());
+  int rc = mcs_modes_at(sp, frfs, n_frfs, centre.data(), centre.size(), modals.data());
+  if (rc) return rc;
+  if (samples.empty()) return MCS_OK;
+  std::lock_guard<std::mutex> lk(c->mu);
+  MCS_CUDA(cudaSetDevice(c->device));
+  DevBuf dm, dq, dr, dout, db, dc;
+  auto release = [&]() {
+    dm.release(); dq.release(); dr.release(); dout.release(); db.release(); dc.release();
+  };
+  if ((rc = dm.ensure(sizeof(mcs_modal) * modals.size())) ||
+      (rc = dq.ensure(sizeof(mcs_lobe_query) * qs.size())) ||
+      (rc = dr.ensure(sizeof(double) * samples.size())) ||
+      (rc = dout.ensure(sizeof(double) * samples.size())) ||
+      (rc = db.ensure(sizeof(int) * qs.size())) || (rc = dc.ensure(sizeof(int) * qs.size()))) {
+    release();
+    return rc;
+  }
+  cudaStream_t st = c->stream;
+  cudaError_t e = cudaMemcpyAsync(dm.p, modals.data(), sizeof(mcs_modal) * modals.size(),
+                                  cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dq.p, qs.data(), sizeof(mcs_lobe_query) * qs.size(),
+                        cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dr.p, samples.data(), sizeof(double) * samples.size(),
+                        cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(db.p, begin.data(), sizeof(int) * qs.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dc.p, count.data(), sizeof(int) * qs.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = (cudaError_t)launch_lobes(st, static_cast<const mcs_modal*>(dm.p),
+                                  static_cast<const mcs_lobe_query*>(dq.p), (int)qs.size(),
+                                  static_cast<const double*>(dr.p), (int)samples.size(),
+                                  static_cast<double*>(dout.p), static_cast<const int*>(db.p),
+                                  static_cast<const int*>(dc.p));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(alim_out, dout.p, sizeof(double) * samples.size(),
+                        cudaMemcpyDeviceToHost, st);
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  release();
+  if (e != cudaSuccess) return fail(MCS_ERR_CUDA, "composite lobes failed: %s", cudaGetErrorString(e));
+  if (e2 != cudaSuccess) return fail(MCS_ERR_CUDA, "composite lobes failed: %s", cudaGetErrorString(e2));
+  for (size_t i = 0; i < samples.size(); i++) {
+    rpm_out[i] = samples[i];
+    if (alim_out[i] == INFINITY) alim_out[i] = 1e3;  // sim.js:282
+  }
+  return MCS_OK;
+}
+
+int mcs_curve_alim(const double* cr, const double* ca, size_t n_curve, const double* rpm,
+                   size_t n, double* out) {
+  if ((n_curve && (!cr || !ca)) || (n && (!rpm || !out)))
+    return fail(MCS_ERR_ARG, "NULL curve, speeds or output");
+  bool ascending = true;
+  for (size_t i = 1; i < n_curve; i++) ascending = ascending && cr[i] >= cr[i - 1];
+  auto seg = [&](size_t i, double v, double& best) {  // segment [i-1, i] if it covers v
+    if (v >= cr[i - 1] && v <= cr[i]) {
+      const double span = cr[i] - cr[i - 1];
+      const double t = (v - cr[i - 1]) / (span != 0 ? span : 1);
+      best = std::min(best, ca[i - 1] + (ca[i] - ca[i - 1]) * t);
+    }
+  };
+  for (size_t r = 0; r < n; r++) {
+    const double v = rpm[r];
+    double best = INFINITY;
+    if (ascending) {  // the covering segments follow the first speed >= v
+      const size_t first = (size_t)(std::lower_bound(cr, cr + n_curve, v) - cr);
+      for (size_t i = std::max<size_t>(first, 1); i < n_curve && cr[i - 1] <= v; i++)
+        seg(i, v, best);
+    } else {
+      for (size_t i = 1; i < n_curve; i++) seg(i, v, best);
+    }
+    out[r] = best;
+  }
+  return MCS_OK;
+}
+
 int mcs_measure_peaks(mcs_ctx* c, mcs_peaks* out) {
   if (!c || !out) return fail(MCS_ERR_ARG, "NULL ctx or output");
   std::lock_guard<std::mutex> lk(c->mu);

@@ -198,6 +198,7 @@ void surrogate_hold(mcs_surrogate* s, int delta);
 int measure_peaks(cudaStream_t st, int sms, void* scratch, double* fp32_tflops,
                   double* fp64_tflops, double* smem_tbps);
 int launch_lobes(cudaStream_t stream, const mcs_modal* modals, const mcs_lobe_query* qs, int n_q,
-                 const double* rpm, int n_rpm, double* out);
+                 const double* rpm, int n_rpm, double* out, const int* q_begin = nullptr,
+                 const int* q_count = nullptr);
 
 }  // namespace mcs

@@ -61,10 +61,15 @@ __device__ __forceinline__ bool key_less(double ka, int ia, double kb, int ib) {
   return ka < kb || (ka == kb && ia < ib);
 }
 
+// Without slices every query is read at all n_rpm speeds, out[q * n_rpm + r]; with slices
+// (q_begin, q_count) query q is read only at rpm[q_begin[q] .. q_begin[q] + q_count[q]) and
+// writes out[r] there (the composite diagram: each node read across its own speeds).
 __global__ void __launch_bounds__(kThreads) lobes_kernel(const mcs_modal* __restrict__ modals,
                                                          const mcs_lobe_query* __restrict__ qs,
                                                          const double* __restrict__ rpm,
-                                                         int n_rpm, double* __restrict__ out) {
+                                                         int n_rpm, double* __restrict__ out,
+                                                         const int* __restrict__ q_begin,
+                                                         const int* __restrict__ q_count) {
   extern __shared__ __align__(16) double sm[];
   double* wc = sm;
   double* al = wc + kMaxNS;
@@ -115,8 +120,10 @@ __global__ void __launch_bounds__(kThreads) lobes_kernel(const mcs_modal* __rest
     al[s] = have ? bestA : -1.0;
     psi[s] = have ? atan(bestK) : 0.0;
   }
-  for (int r = threadIdx.x; r < n_rpm; r += kThreads)
-    out[(size_t)blockIdx.x * n_rpm + r] = INFINITY;
+  const int r0 = q_begin ? q_begin[blockIdx.x] : 0;
+  const int r1 = q_begin ? r0 + q_count[blockIdx.x] : n_rpm;
+  double* outq = q_begin ? out : out + (size_t)blockIdx.x * n_rpm;
+  for (int r = r0 + threadIdx.x; r < r1; r += kThreads) outq[r] = INFINITY;
   __syncthreads();
 
   for (int j = 0; j < Q.lobes; j++) {
@@ -165,7 +172,7 @@ __global__ void __launch_bounds__(kThreads) lobes_kernel(const mcs_modal* __rest
     __syncthreads();
     const int n = s_valid;
     // alimAt (sld.js:64-76): every consecutive pair [a, b] with a.rpm <= rpm <= b.rpm
-    for (int r = threadIdx.x; r < n_rpm; r += kThreads) {
+    for (int r = r0 + threadIdx.x; r < r1; r += kThreads) {
       const double v = rpm[r];
       int lo = 0, hi = n;  // lower bound: first key >= v
       while (lo < hi) {
@@ -179,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) lobes_kernel(const mcs_modal* __rest
         if (key[mid] <= v) lo = mid + 1; else hi = mid;
       }
       const int upper = lo;
-      double best = out[(size_t)blockIdx.x * n_rpm + r];
+      double best = outq[r];
       for (int i = max(lower, 1); i <= min(upper, n - 1); i++) {
         const double ar = key[i - 1], br = key[i];
         const double aa = al[kid[i - 1]], ba = al[kid[i]];
@@ -187,7 +194,7 @@ __global__ void __launch_bounds__(kThreads) lobes_kernel(const mcs_modal* __rest
         const double t = (v - ar) / (span != 0 ? span : 1);
         best = fmin(best, aa + (ba - aa) * t);
       }
-      out[(size_t)blockIdx.x * n_rpm + r] = best;
+      outq[r] = best;
     }
     __syncthreads();
   }
@@ -198,12 +205,14 @@ __global__ void __launch_bounds__(kThreads) lobes_kernel(const mcs_modal* __rest
 constexpr int kLobeSmem = 3 * kMaxNS * 8 + kSortN * 8 + kSortN * 4;
 
 int launch_lobes(cudaStream_t stream, const mcs_modal* modals, const mcs_lobe_query* qs, int n_q,
-                 const double* rpm, int n_rpm, double* out) {
+                 const double* rpm, int n_rpm, double* out, const int* q_begin,
+                 const int* q_count) {
   cudaError_t e = cudaFuncSetAttribute(lobes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kLobeSmem);
   if (e != cudaSuccess) return (int)e;
   if (n_q == 0) return 0;
-  lobes_kernel<<<n_q, kThreads, kLobeSmem, stream>>>(modals, qs, rpm, n_rpm, out);
+  lobes_kernel<<<n_q, kThreads, kLobeSmem, stream>>>(modals, qs, rpm, n_rpm, out, q_begin,
+                                                     q_count);
   return (int)cudaGetLastError();
 }
 

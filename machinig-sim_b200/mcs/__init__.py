@@ -17,14 +17,14 @@ from ._abi import (CHATTER_IDX, DEFAULTS, make_material, make_modal, make_opts, 
                    make_tool)
 from ._lib import (Context, Job, MCSError, Plan, Surrogate, default_context,
                    default_guide_opts, default_train_opts, load)
-from .sld import lobeLimit, lobeLimits
+from .sld import alimAt, compositeLobes, lobeLimit, lobeLimits
 from .spindle import Spindle, lobe_speeds, sweep_points, tool_model
 from .stabtd import chatterAt, chatterIndex, timeDomainLimit, timeDomainLimits
 from .worker import StabWorker
 
 __all__ = [
     "CHATTER_IDX", "DEFAULTS", "Context", "Job", "MCSError", "Plan", "Spindle", "StabWorker",
-    "Surrogate", "lobe_speeds", "sweep_points", "tool_model",
+    "Surrogate", "alimAt", "compositeLobes", "lobe_speeds", "sweep_points", "tool_model",
     "chatterAt", "chatterIndex", "default_context", "default_guide_opts",
     "default_train_opts", "load", "lobeLimit", "lobeLimits",
     "make_material", "make_modal", "make_opts", "make_setup", "make_tool", "timeDomainLimit",

@@ -28,7 +28,7 @@ EXPORTS = (
     "mcs_surrogate_destroy", "mcs_surrogate_train", "mcs_surrogate_predict", "mcs_surrogate_grad",
     "mcs_surrogate_get_params", "mcs_surrogate_set_params", "mcs_solve_guided",
     "mcs_plan_create_guided", "mcs_plan_guide_info", "mcs_tune", "mcs_measure_peaks",
-    "mcs_modes_at",
+    "mcs_modes_at", "mcs_lobes_composite", "mcs_curve_alim",
 )
 _VOID = ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free",
          "mcs_default_train_opts", "mcs_default_guide_opts")
@@ -100,6 +100,9 @@ def load(path: Path | str | None = None):
         L.mcs_plan_guide_info.argtypes = [vp, vp]
         L.mcs_measure_peaks.argtypes = [vp, P(A.Peaks)]
         L.mcs_modes_at.argtypes = [P(A.Spindle), vp, C.c_size_t, vp, C.c_size_t, vp]
+        L.mcs_lobes_composite.argtypes = [vp, P(A.Spindle), vp, C.c_size_t, P(A.LobeQuery), vp,
+                                          vp, C.c_size_t, P(C.c_size_t)]
+        L.mcs_curve_alim.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp]
         for name in EXPORTS:
             if name not in _VOID:
                 getattr(L, name).restype = C.c_int
@@ -309,6 +312,18 @@ class Context:
         check(self._L.mcs_lobes_alim(self._h, _ptr(m), len(m), C.cast(q, C.c_void_p),
                                      len(queries), _ptr(r), len(r), _ptr(out)))
         return out
+
+    def lobes_composite(self, spindle, base: A.LobeQuery):
+        """(rpm, alim) of the speed-dependent composite diagram (mcs_lobes_composite)."""
+        n = C.c_size_t()
+        F = A.array_of(A.SpeedFrf, spindle.frfs)
+        args = (self._h, C.byref(spindle.record), C.cast(F, C.c_void_p), len(spindle.frfs),
+                C.byref(base))
+        check(self._L.mcs_lobes_composite(*args, None, None, 0, C.byref(n)))
+        rpm = np.zeros(max(1, n.value))
+        alim = np.zeros(max(1, n.value))
+        check(self._L.mcs_lobes_composite(*args, _ptr(rpm), _ptr(alim), n.value, C.byref(n)))
+        return rpm[: n.value], alim[: n.value]
 
     def measure_peaks(self) -> dict:
         """Measured FP32/FP64 FMA rates [TFLOP/s] and shared-memory bandwidth [TB/s] of this

@@ -5,6 +5,10 @@ evaluated at given spindle speeds in one call (mcs_lobes_alim).
                      "lobes": 30, "rpmMin": 2000, "rpmMax": 40000}, rpms)
 
 equals ``[alimAt(stabilityLobes(params), s) for s in rpms]`` of the reference.
+
+With speed-dependent dynamics the chart's diagram is a composite (Simulator.lobes,
+sim.js:262-287): compositeLobes builds it from one GPU diagram per 1000 rpm with that
+speed's modes, and alimAt reads any lobe list per pixel (charts.js:170-185).
 """
 from __future__ import annotations
 
@@ -13,7 +17,7 @@ from typing import Any, Mapping, Sequence
 import numpy as np
 
 from . import _abi as A
-from ._lib import Context, default_context
+from ._lib import Context, _ptr, check, default_context, load
 
 
 def lobe_query(params: Mapping[str, Any], modal_index: int = 0) -> A.LobeQuery:
@@ -37,3 +41,28 @@ def lobeLimits(params_list: Sequence[Mapping[str, Any]], rpm, *,
     modals = [A.make_modal(p) for p in params_list]
     qs = [lobe_query(p, i) for i, p in enumerate(params_list)]
     return c.lobes_alim(modals, qs, np.atleast_1d(rpm))
+
+
+def compositeLobes(spindle, params: Mapping[str, Any], *, ctx: Context | None = None):
+    """The chart's speed-dependent diagram [[{rpm, alim}]] (sim.js:269-285): params gives N,
+    Ktc, Krc, phiSt, phiEx, lobes (30) and rpmMin/rpmMax (2000/40000); the modes come from
+    the spindle model (mcs.spindle.Spindle) at each node's centre."""
+    c = ctx if ctx is not None else default_context()
+    p = {"lobes": 30, "rpmMin": 2000, "rpmMax": 40000, **dict(params)}
+    rpm, alim = c.lobes_composite(spindle, lobe_query(p))
+    return [[{"rpm": float(r), "alim": float(a)} for r, a in zip(rpm, alim)]]
+
+
+def alimAt(lobes, rpm):
+    """alimAt (sld.js:64-76) of lobe lists [[{rpm, alim}]] at each speed in rpm: the minimum
+    over the lobes of the interpolation on the segments covering the speed (mcs_curve_alim,
+    host arithmetic); inf where none does.  A scalar speed gives a float."""
+    r = np.ascontiguousarray(np.atleast_1d(rpm), dtype=np.float64)
+    best = np.full(len(r), np.inf)
+    out = np.zeros(max(1, len(r)))
+    for lobe in lobes:
+        cr = np.ascontiguousarray([pt["rpm"] for pt in lobe], dtype=np.float64)
+        ca = np.ascontiguousarray([pt["alim"] for pt in lobe], dtype=np.float64)
+        check(load().mcs_curve_alim(_ptr(cr), _ptr(ca), len(cr), _ptr(r), len(r), _ptr(out)))
+        best = np.minimum(best, out[: len(r)])
+    return float(best[0]) if np.ndim(rpm) == 0 else best

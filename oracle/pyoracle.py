@@ -348,3 +348,29 @@ def modes_at(spindle: A.Spindle, speeds, frfs=()) -> np.ndarray:
     lib().or_modes_at(C.byref(spindle), C.cast(F, C.c_void_p), len(frfs), _dptr(S), len(S),
                       C.c_void_p(out.ctypes.data))
     return out[: len(S)]
+
+
+LOBE_NODE, LOBE_STEP = 1000, 25  # src/sim.js:37
+
+
+def composite_lobes(spindle: A.Spindle, params: dict, frfs=()):
+    """Simulator.lobes for speed-dependent dynamics (src/sim.js:269-285): a diagram per
+    LOBE_NODE with the modes at the node's centre, each read every LOBE_STEP across its own
+    node, Infinity read as 1e3; returns [curve]."""
+    base = {"lobes": 30, "rpmMin": 2000, "rpmMax": 40000, **params}
+    curve = []
+    lo, hi = base["rpmMin"] * 0.8, base["rpmMax"] * 1.1
+    S0 = lo
+    while S0 < hi:
+        m = modes_at(spindle, [S0 + LOBE_NODE / 2], frfs)[0]
+        own = {**base, "rpmMin": S0, "rpmMax": S0 + LOBE_NODE, "k": 0, "fn": 0, "zeta": 0,
+               "modesX": [{"k": x["k"], "fn": x["fn"], "zeta": x["zeta"]} for x in m["x"][: m["nx"]]],
+               "modesY": [{"k": y["k"], "fn": y["fn"], "zeta": y["zeta"]} for y in m["y"][: m["ny"]]]}
+        lob = stabilityLobes(own)
+        S = S0
+        while S < min(hi, S0 + LOBE_NODE):
+            a = alimAt(lob, S)
+            curve.append({"rpm": S, "alim": 1e3 if a == math.inf else a})
+            S += LOBE_STEP
+        S0 += LOBE_NODE
+    return [curve]

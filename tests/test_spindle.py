@@ -122,3 +122,24 @@ def test_bad_spindle_models_are_rejected():
             two_dof={"mTool": 0.0, "mSp": 1.0}).modes_at([1000.0])
     with pytest.raises(MCSError):
         _sp({"k": 1e4, "fn": 2000, "zeta": 0.04}).modes_at([float("nan")])
+
+
+def test_curve_alim_matches_the_reference_read_out(oracle):
+    """mcs_curve_alim (the chart's per-pixel alimAt, charts.js:170-185) against the oracle's
+    alimAt on lobes of its own stabilityLobes, ascending and with an unsorted polyline."""
+    import mcs
+
+    params = {"N": 3, "Ktc": 2100, "Krc": 850, "phiSt": math.pi / 2, "phiEx": math.pi,
+              "lobes": 12, "rpmMin": 2000, "rpmMax": 40000, "k": 1.1e4, "fn": 1900,
+              "zeta": 0.03}
+    lobes = oracle.stabilityLobes(params)
+    rpm = np.concatenate([np.linspace(1500, 42000, 400), [lobes[0][0]["rpm"]]])
+    got = mcs.alimAt(lobes, rpm)
+    ref = np.array([oracle.alimAt(lobes, r) for r in rpm])
+    assert np.array_equal(np.isfinite(got), np.isfinite(ref))
+    assert np.array_equal(got[np.isfinite(ref)], ref[np.isfinite(ref)])
+    odd = [[{"rpm": 3.0, "alim": 1.0}, {"rpm": 1.0, "alim": 2.0}, {"rpm": 2.0, "alim": 3.0},
+            {"rpm": 4.0, "alim": 5.0}]]
+    for r in (0.5, 1.0, 1.5, 2.0, 2.5, 3.5, 4.0, 5.0):
+        a, b = mcs.alimAt(odd, r), oracle.alimAt(odd, r)
+        assert (a == b) or (math.isinf(a) and math.isinf(b)), (r, a, b)
