@@ -534,8 +534,15 @@ def ours(args) -> int:
     def measure(name: str, precisions, steps: int, warmup: int, e2e_steps: int, cpu: bool):
         """One workload: every precision timed as a plan, the headline precision also end
         to end; on rank 0 of a 1-GPU run the host FP64 baseline and the accuracy."""
-        wl = make_workload(name, rank, args.points)
-        pts_total = wl.n * world
+        if args.strong and world > 1:  # one batch split by the library's cost-balanced shards
+            from mcs import dist as D
+
+            full = make_workload(name, 0, args.points)
+            wl = full.subset(D.library_shards(full, world)[rank])
+            pts_total = full.n
+        else:  # every rank its own seeded batch (weak scaling)
+            wl = make_workload(name, rank, args.points)
+            pts_total = wl.n * world
         var = {p: timed(wl, p, steps, warmup) for p in precisions}
         head = var[precisions[0]]
         e2e = None
@@ -596,7 +603,8 @@ def ours(args) -> int:
         line = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True,
+            "scaling": "strong" if args.strong and world > 1 else "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32" else "f64",
             "data": "synthetic (seeded; no public dataset exists for this path)",
             "config": head["config"],
@@ -647,6 +655,9 @@ def main(argv=None) -> int:
                     help="fixed schedule (shared-memory size classes); 0: autotune")
     ap.add_argument("--coop-warps", type=int, default=-1,
                     help="warps sharing each heaviest point's bisection (1: off; -1: default)")
+    ap.add_argument("--strong", action="store_true",
+                    help="N > 1: split one batch over the ranks (mcs_shard) instead of one "
+                         "batch per rank")
     ap.add_argument("--serial-trials", action="store_true",
                     help="one bisection trial per warp at a time (same results)")
     a = ap.parse_args(argv)

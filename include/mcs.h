@@ -212,6 +212,29 @@ int mcs_solve(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs_
               mcs_result* out);
 
 /*
+ * Several devices: the batch of mcs_solve split over the contexts ctxs[0..n_ctx) (one per
+ * device, or several on one device), solved at once by one host thread per context, and the
+ * results concatenated in input order into out[n_points].  Points are independent, so the
+ * shards need no exchange: no peer memory, no collective.  The split is mcs_shard's.  On a
+ * failure every shard still finishes; the first failing shard's status and message are
+ * returned.  The multi-GPU form of the Worker's sweep (stabworker.js:6-14).
+ */
+int mcs_solve_multi(mcs_ctx* const* ctxs, size_t n_ctx, const mcs_setup* setups,
+                    size_t n_setups, const mcs_modal* modals, size_t n_modals,
+                    const mcs_point* points, size_t n_points, const mcs_opts* opts,
+                    mcs_result* out);
+/*
+ * The split of mcs_solve_multi: each point's estimated cost (steps per trial x trials x the
+ * slice evaluations a step visits, from the same FP64 preparation the solve uses) into
+ * cost[i] (NULL allowed), and a longest-first greedy assignment (each point in decreasing
+ * cost to the least-loaded shard, ties to the lower index) into shard_of[i] in
+ * [0, n_shards).  Host arithmetic; no device needed.
+ */
+int mcs_shard(const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+              size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* opts,
+              size_t n_shards, int32_t* shard_of, double* cost);
+
+/*
  * Batched chatterAt (stabtd.js:14-22): one trial per entry of trials[], returning the
  * chatter index parts and the decision.  Used to replay decisions at given depths.
  */

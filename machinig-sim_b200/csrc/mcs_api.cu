@@ -11,7 +11,9 @@
 #include <limits>
 #include <mutex>
 #include <numeric>
+#include <queue>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mcs_internal.h"
@@ -979,6 +981,75 @@ int mcs_solve(mcs_ctx* c, const mcs_setup* setups, size_t n_setups, const mcs_mo
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (!rc && e != cudaSuccess) rc = fail(MCS_ERR_CUDA, "solve failed: %s", cudaGetErrorString(e));
   return rc;
+}
+
+int mcs_shard(const mcs_setup* setups, size_t n_setups, const mcs_modal* modals,
+              size_t n_modals, const mcs_point* points, size_t n_points, const mcs_opts* o,
+              size_t n_shards, int32_t* shard_of, double* cost_out) {
+  if (n_shards < 1 || n_shards > 4096) return fail(MCS_ERR_ARG, "n_shards out of range [1, 4096]");
+  if (n_points && !shard_of) return fail(MCS_ERR_ARG, "shard_of is NULL");
+  int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
+  if (rc) return rc;
+  std::vector<double> cost(n_points);
+  for (size_t i = 0; i < n_points; i++) {
+    Prepared pr;
+    rc = prepare_point(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,
+                       o->a_max, pr);
+    if (rc) return fail(rc, "point %zu: %s", i, g_last_error.c_str());
+    cost[i] = pr.cost;
+  }
+  std::vector<size_t> order(n_points);
+  std::iota(order.begin(), order.end(), size_t(0));
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+  // least-loaded shard first, the lower index among equal loads
+  using Load = std::pair<double, size_t>;
+  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+  for (size_t k = 0; k < n_shards; k++) heap.push({0.0, k});
+  for (size_t i : order) {
+    const Load l = heap.top();
+    heap.pop();
+    shard_of[i] = (int32_t)l.second;
+    heap.push({l.first + cost[i], l.second});
+  }
+  if (cost_out) std::copy(cost.begin(), cost.end(), cost_out);
+  return MCS_OK;
+}
+
+int mcs_solve_multi(mcs_ctx* const* ctxs, size_t n_ctx, const mcs_setup* setups,
+                    size_t n_setups, const mcs_modal* modals, size_t n_modals,
+                    const mcs_point* points, size_t n_points, const mcs_opts* o,
+                    mcs_result* out) {
+  if (!ctxs || n_ctx == 0) return fail(MCS_ERR_ARG, "no contexts");
+  for (size_t k = 0; k < n_ctx; k++)
+    if (!ctxs[k]) return fail(MCS_ERR_ARG, "context %zu is NULL", k);
+  if (n_points && !out) return fail(MCS_ERR_ARG, "out is NULL");
+  std::vector<int32_t> shard_of(n_points);
+  int rc = mcs_shard(setups, n_setups, modals, n_modals, points, n_points, o, n_ctx,
+                     shard_of.data(), nullptr);
+  if (rc) return rc;
+  std::vector<std::vector<size_t>> idx(n_ctx);
+  for (size_t i = 0; i < n_points; i++) idx[shard_of[i]].push_back(i);
+  std::vector<int> status(n_ctx, MCS_OK);
+  std::vector<std::string> message(n_ctx);
+  std::vector<std::vector<mcs_result>> res(n_ctx);
+  auto work = [&](size_t k) {
+    std::vector<mcs_point> pts(idx[k].size());
+    for (size_t j = 0; j < pts.size(); j++) pts[j] = points[idx[k][j]];
+    res[k].resize(pts.size());
+    status[k] = mcs_solve(ctxs[k], setups, n_setups, modals, n_modals, pts.data(), pts.size(), o,
+                          res[k].data());
+    if (status[k]) message[k] = g_last_error;  // this thread's message
+  };
+  std::vector<std::thread> pool;
+  for (size_t k = 1; k < n_ctx; k++) pool.emplace_back(work, k);
+  work(0);
+  for (std::thread& t : pool) t.join();
+  for (size_t k = 0; k < n_ctx; k++)
+    if (status[k]) return fail(status[k], "shard %zu: %s", k, message[k].c_str());
+  for (size_t k = 0; k < n_ctx; k++)
+    for (size_t j = 0; j < idx[k].size(); j++) out[idx[k][j]] = res[k][j];
+  return MCS_OK;
 }
 
 int mcs_chatter_at(mcs_ctx* c, const mcs_setup* setups, size_t n_setups,

@@ -15,7 +15,7 @@ All compute runs in the CUDA library; a missing library or device raises.
 """
 from ._abi import (CHATTER_IDX, DEFAULTS, make_material, make_modal, make_opts, make_setup,
                    make_tool)
-from ._lib import (Context, Job, MCSError, Plan, Surrogate, default_context,
+from ._lib import (Context, Job, MCSError, Plan, Surrogate, default_context, shard, solve_multi,
                    default_guide_opts, default_train_opts, load)
 from .sld import alimAt, compositeLobes, lobeLimit, lobeLimits
 from .spindle import Spindle, lobe_speeds, sweep_points, tool_model
@@ -24,7 +24,7 @@ from .worker import StabWorker
 
 __all__ = [
     "CHATTER_IDX", "DEFAULTS", "Context", "Job", "MCSError", "Plan", "Spindle", "StabWorker",
-    "Surrogate", "alimAt", "compositeLobes", "lobe_speeds", "sweep_points", "tool_model",
+    "Surrogate", "alimAt", "shard", "solve_multi", "compositeLobes", "lobe_speeds", "sweep_points", "tool_model",
     "chatterAt", "chatterIndex", "default_context", "default_guide_opts",
     "default_train_opts", "load", "lobeLimit", "lobeLimits",
     "make_material", "make_modal", "make_opts", "make_setup", "make_tool", "timeDomainLimit",

@@ -28,7 +28,7 @@ EXPORTS = (
     "mcs_surrogate_destroy", "mcs_surrogate_train", "mcs_surrogate_predict", "mcs_surrogate_grad",
     "mcs_surrogate_get_params", "mcs_surrogate_set_params", "mcs_solve_guided",
     "mcs_plan_create_guided", "mcs_plan_guide_info", "mcs_tune", "mcs_measure_peaks",
-    "mcs_modes_at", "mcs_lobes_composite", "mcs_curve_alim",
+    "mcs_modes_at", "mcs_lobes_composite", "mcs_curve_alim", "mcs_solve_multi", "mcs_shard",
 )
 _VOID = ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free",
          "mcs_default_train_opts", "mcs_default_guide_opts")
@@ -103,6 +103,8 @@ def load(path: Path | str | None = None):
         L.mcs_lobes_composite.argtypes = [vp, P(A.Spindle), vp, C.c_size_t, P(A.LobeQuery), vp,
                                           vp, C.c_size_t, P(C.c_size_t)]
         L.mcs_curve_alim.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp]
+        L.mcs_solve_multi.argtypes = [vp, C.c_size_t] + batch[1:] + [vp]
+        L.mcs_shard.argtypes = batch[1:] + [C.c_size_t, vp, vp]
         for name in EXPORTS:
             if name not in _VOID:
                 getattr(L, name).restype = C.c_int
@@ -441,3 +443,25 @@ def default_context(device: int = 0) -> Context:
             _DEFAULT.setdefault(device, ctx)
             ctx = _DEFAULT[device]
     return ctx
+
+
+def shard(setups, modals, points, opts: A.Opts, n_shards: int):
+    """(shard of each point, cost of each point) of mcs_shard: the split mcs_solve_multi
+    uses (host arithmetic, no device)."""
+    b = Batch(setups, modals, points)
+    n = len(b.points)
+    of = np.zeros(max(1, n), dtype=np.int32)
+    cost = np.zeros(max(1, n), dtype=np.float64)
+    check(load().mcs_shard(*b.args(), C.byref(opts), int(n_shards), _ptr(of), _ptr(cost)))
+    return of[:n], cost[:n]
+
+
+def solve_multi(contexts: Sequence["Context"], setups, modals, points, opts: A.Opts):
+    """mcs_solve over several contexts at once (mcs_solve_multi), results in input order."""
+    b = Batch(setups, modals, points)
+    n = len(b.points)
+    hs = (C.c_void_p * len(contexts))(*[c._h.value for c in contexts])
+    out = np.zeros(max(1, n), dtype=A.RESULT_DTYPE)
+    check(load().mcs_solve_multi(C.cast(hs, C.c_void_p), len(contexts), *b.args(),
+                                 C.byref(opts), _ptr(out)))
+    return out[:n]

@@ -44,6 +44,15 @@ def shard(cost: np.ndarray, world: int) -> list[np.ndarray]:
     return [np.sort(np.array(p, dtype=np.int64)) for p in parts]
 
 
+def library_shards(workload, world: int) -> list[np.ndarray]:
+    """The library's split (mcs_shard, the one mcs_solve_multi uses): point indices of each
+    of `world` shards, from the FP64 preparation's cost of every point (host only)."""
+    from ._lib import shard as lib_shard
+
+    of, _ = lib_shard(workload.setups, workload.modals, workload.points, workload.opts, world)
+    return [np.flatnonzero(of == r) for r in range(world)]
+
+
 def gather_results(local_idx: np.ndarray, local_res: np.ndarray, n_total: int, dist,
                    group=None) -> np.ndarray | None:
     """Rank 0 receives every shard's result records in the original point order."""

@@ -180,3 +180,22 @@ def test_lobe_limit_mirror(ctx, oracle, modal):
     lobes = oracle.stabilityLobes(p)
     want = [oracle.alimAt(lobes, r) for r in rpm]
     assert np.allclose(got, want, rtol=1e-10)
+
+
+def test_solve_multi_equals_solve(ctx):
+    """mcs_solve_multi over one context, and over two contexts on the same device (one host
+    thread each), gives mcs_solve's records in input order."""
+    import mcs
+    from mcs import workloads as W
+
+    wl = W.hetero(n=300, first_seed=55)
+    wl.opts.revs = 20
+    ref = ctx.solve(wl.setups, wl.modals, wl.points, wl.opts)
+    one = mcs.solve_multi([ctx], wl.setups, wl.modals, wl.points, wl.opts)
+    assert one.tobytes() == ref.tobytes()
+    c2 = mcs.Context(0)
+    try:
+        two = mcs.solve_multi([ctx, c2], wl.setups, wl.modals, wl.points, wl.opts)
+    finally:
+        c2.close()
+    assert two.tobytes() == ref.tobytes()
