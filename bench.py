@@ -384,6 +384,39 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool, repeats: 
     return res
 
 
+def worker_latency(ctx, torch, precision: str, repeats: int = 3) -> dict:
+    """Latency of the stability Worker's request (main.js:494-501): the 18 log-spaced lobe
+    speeds of one setup, each with its own modes (the spindle model), through the blocking
+    call mcs_solve, with and without several warps sharing each point's bisection."""
+    from mcs import _abi as A
+    from mcs import workloads as W
+
+    wl = W.spindle_sweep()
+    sel = wl.points["setup"] == 0
+    pts = wl.points[sel]
+    out = {"workload": f"{int(sel.sum())} lobe speeds 4000-30000 rpm with speed-dependent "
+                       "modes, reference options ([0.05, 20] x 8, 120 revs)",
+           "precision": precision}
+    res = None
+    for name, cw in (("one_warp", 1), ("multi_warp", 0)):
+        o = A.Opts.from_buffer_copy(bytes(wl.opts))
+        o.precision = A.precision_code(precision)
+        o.coop_warps = cw
+        ctx.solve(wl.setups, wl.modals, pts, o)  # warm-up
+        ts = []
+        for _ in range(repeats):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = ctx.solve(wl.setups, wl.modals, pts, o)
+            ts.append(1e3 * (time.perf_counter() - t0))
+        out[f"{name}_ms"] = float(np.median(ts))
+        res = r if name == "one_warp" else res
+        if name == "multi_warp":
+            assert r.tobytes() == res.tobytes(), "multi-warp results differ"
+    out["speedup"] = out["one_warp_ms"] / out["multi_warp_ms"]
+    return out
+
+
 def make_workload(name: str, rank: int, points: int = 0):
     from mcs import workloads as W
 
@@ -600,6 +633,8 @@ def ours(args) -> int:
         guided = (guided_serve(ctx, torch, stream, flush, device, args.no_cpu,
                                args.guided_repeats)
                   if world == 1 and not args.no_guided else None)
+        latency = (worker_latency(ctx, torch, args.precision)
+                   if world == 1 and not args.no_latency else None)
         line = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
@@ -622,6 +657,7 @@ def ours(args) -> int:
             "workloads": {"hetero": summarize("hetero", hetero, args.precision)}
             if hetero else None,
             "guided": guided,
+            "worker_latency": latency,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -649,6 +685,8 @@ def main(argv=None) -> int:
                     help="skip the surrogate-guided serving leg")
     ap.add_argument("--no-hetero", action="store_true", help="skip the hetero workload leg")
     ap.add_argument("--guided-repeats", type=int, default=5)
+    ap.add_argument("--no-latency", action="store_true",
+                    help="skip the latency of the Worker's 18-speed request")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "hetero"],
                     help="sweep (the headline) or the heterogeneous batch")
     ap.add_argument("--max-buckets", type=int, default=0,

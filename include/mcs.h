@@ -124,9 +124,11 @@ typedef struct {
                               1: one trial at a time.  Results are identical either way. */
   int32_t coop_warps;      /* schedule: the heaviest points (up to one per SM) share their
                               bisection among this many warps of one block, each running one
-                              trial of the next levels speculatively (2..8; 0: 8, narrowed to
-                              4 or 3 where 8 rings do not fit in shared memory; 1: off).
-                              Plain solves only.  Results are identical either way. */
+                              trial of the next levels speculatively (2..8, narrowed to 4 or 3
+                              where the rings do not fit in shared memory; 1: off; 0: 8 for
+                              batches of at most 4 points per SM, where the slowest points'
+                              serial bisections are the whole call, else off).  Plain solves
+                              only.  Results are identical either way. */
 } mcs_opts;
 
 #define MCS_MAX_BUCKETS 32
@@ -434,6 +436,103 @@ typedef struct {
  * measurements).  Output sets always give ny explicitly. */
 int mcs_modes_at(const mcs_spindle* spindle, const mcs_speed_frf* frfs, size_t n_frfs,
                  const double* S, size_t n_speeds, mcs_modal* out);
+
+/* ------------------------------------------------------------------ cutting engines
+ * A batch of time-domain cutting engines on one device: class CuttingEngine of
+ * src/cutting.js:21-321 with every term its run() loop gives a cut -- the flutes' force law
+ * with size effect, process damping, runout and a general edge profile (:115-118), the
+ * axial force and the torque, the end (bottom) edges (:130-143, 215-237), a compliant thin
+ * wall (:88-94, 256-264), the modal integration, the once-per-tooth samples, the decimated
+ * force and position history (:288-292) and the statistics takeStats() returns.  Every
+ * engine keeps its state on the device between runs, as the JS object does between run()
+ * calls: the Simulator's real-time playback (Simulator.step, sim.js:351-420) configures an
+ * engine for a speed, sets each substep's engagement and runs it for the substep's steps
+ * (the dynamics budget of worker.js:22-32); coefficient identification (identify.js:26-40)
+ * and validation (validate.js:76-100) run many rigid-tool engines in one launch.  FP64
+ * arithmetic with the surface ring in float (the reference's Float32Array).  Wall samples
+ * and chip events (inputs of the roughness and chip models, outside this library) are not
+ * produced.  One warp simulates one engine.
+ */
+#define MCS_END_BINS 36
+#define MCS_END_RINGS 6
+#define MCS_MAX_SLICES 64
+#define MCS_ENGINE_HIST 4096 /* history ring (cutting.js:28) */
+#define MCS_ENGINE_TS 64     /* once-per-tooth sample ring (cutting.js:29) */
+
+typedef struct mcs_engine mcs_engine;
+
+/* configure(tool, modal, mat, S, fnMax) (cutting.js:39-82). */
+typedef struct {
+  mcs_tool tool;      /* runout and its phase as given */
+  mcs_modal modal;
+  double Ktc, Krc, Kac; /* shearing coefficients [N/mm^2] */
+  double Kte, Kre, Kae; /* edge coefficients [N/mm] */
+  double mc, Ci;      /* size-effect exponent, process-damping coefficient [N/m] */
+  double S;           /* spindle speed [rpm] */
+  double fn_max;      /* highest frequency to resolve besides the modes [Hz] (0) */
+  int32_t nonlinear;  /* size effect and process damping (tool.nonlinear) */
+  int32_t decim;      /* history every decim steps: 0 = round(spt / 40) (cutting.js:77) */
+} mcs_engine_config;
+
+/* One substep's engagement: setEngagement (:98-124), setEndEngagement (:130-143), setWork
+ * (:88-94) and setWear (:85) together. */
+typedef struct {
+  float Hb[MCS_BINS];    /* material height at the periphery per angle bin [mm] */
+  double ux, uy;         /* unit feed direction */
+  double fz, tip_z, ap;  /* feed per tooth, tool tip height, engaged axial depth [mm] */
+  int32_t profile;       /* 1: slice_r / slice_kap give each slice's radius [mm] and the
+                            cosine of its edge angle (a general edge profile rAt) */
+  int32_t wear;          /* 1: Kte / Kre below replace the material's (setWear) */
+  double Kte, Kre;
+  double slice_r[MCS_MAX_SLICES], slice_kap[MCS_MAX_SLICES];
+  float Eb[MCS_END_BINS * MCS_END_RINGS]; /* material depth above the end face [bin][ring] */
+  double fza, end_r;     /* axial feed per tooth (0: end edges idle), end-face radius [mm] */
+  double ring_z[MCS_END_RINGS];  /* tip profile z at each ring's radius r_j, and at */
+  double ring_zo[MCS_END_RINGS]; /*   min(end_r, r_j + dr/4) and max(0, r_j - dr/4), */
+  double ring_zi[MCS_END_RINGS]; /*   dr = end_r / rings (the slope, cutting.js:135-137) */
+  double wall_k, wall_m, wall_zeta; /* thin-wall mode [N/mm], [kg]; wall_k = 0: rigid */
+  double wall_nx, wall_ny;          /* its unit normal */
+} mcs_engagement;
+
+/* takeStats() (cutting.js:320-323): sums since the last take, then reset. */
+typedef struct {
+  double n, sumF, maxF, sumFx, sumFy, sumFz, maxFz, sumT, maxT, sumX, sumY;
+  double minX, maxX, minY, maxY, sumZc, wZc, sumW, maxW, sumHb, sumB, sumRb, engTeeth;
+} mcs_engine_stats;
+
+/* The state an engine carries between runs. */
+typedef struct {
+  double x, y, vx, vy;   /* tool position [m] and velocity [m/s] */
+  double t;              /* time [s] */
+  double w, wv;          /* wall deflection [m] and velocity */
+  double dt;             /* step [s] */
+  double run_mean_w;     /* mean wall deflection over the last run [m] */
+  int32_t pr;            /* step within the revolution */
+  int32_t nz;            /* slices engaged */
+  int32_t steps_per_tooth, steps_per_rev, max_slices, decim;
+  uint64_t step_count;
+} mcs_engine_state;
+
+int mcs_engine_create(mcs_ctx* ctx, size_t n_engines, mcs_engine** engine);
+int mcs_engine_destroy(mcs_engine* engine);
+/* cfg[n_engines]: a fresh engine each (the surface, modes, samples and statistics cleared). */
+int mcs_engine_configure(mcs_engine* engine, const mcs_engine_config* cfg);
+/* g[n_engines]: every engine's engagement for its next runs. */
+int mcs_engine_set_engagement(mcs_engine* engine, const mcs_engagement* g);
+/* xv[n_engines][4] = x, y [m], vx, vy [m/s]: the state set from outside (e.x = ..., the kick
+ * of chatterAt); the next run moves the change into the first modes (cutting.js:163-164). */
+int mcs_engine_set_state(mcs_engine* engine, const double* xv);
+/* steps[n_engines] steps of each engine, all in one launch (0: that engine idles). */
+int mcs_engine_run(mcs_engine* engine, const int64_t* steps);
+int mcs_engine_take_stats(mcs_engine* engine, mcs_engine_stats* out);
+int mcs_engine_get_state(mcs_engine* engine, mcs_engine_state* out);
+/* The force and position history ring of each engine: out[e][c][MCS_ENGINE_HIST] for
+ * c = Fx, Fy, Fz [N], x, y [um]; head[e] = the next write index, count[e] = samples written
+ * (either may be NULL).  reset_history (validate.js:81) empties the rings. */
+int mcs_engine_history(mcs_engine* engine, float* out, int32_t* head, int64_t* count);
+int mcs_engine_reset_history(mcs_engine* engine);
+/* chatterIndex() (cutting.js:299-318) of each engine: out[e][3] = index, amp, once. */
+int mcs_engine_chatter_index(mcs_engine* engine, double* out);
 
 /* ------------------------------------------------------------------ measurement
  * Peak rates of the context's device, measured with CUDA events on its stream: FP32 and

@@ -19,7 +19,7 @@ ROOT = HERE.parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libmcs.so"
 SOURCES = ["mcs_kernels.cu", "mcs_lobes.cu", "mcs_surrogate.cu", "mcs_probe.cu", "mcs_spindle.cpp",
-           "mcs_api.cu"]
+           "mcs_engine.cu", "mcs_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -38,6 +38,8 @@ UNITS = [("mcs_kernels.cu", "mcs_kernels_f32.o", ["-DMCS_PREC=32"]),
          ("mcs_surrogate.cu", "mcs_surrogate.o", []),
          ("mcs_probe.cu", "mcs_probe.o", []),
          ("mcs_spindle.cpp", "mcs_spindle.o", []),
+         # separately rounded products and sums, as the reference's JavaScript evaluates
+         ("mcs_engine.cu", "mcs_engine.o", ["-fmad=false"]),
          ("mcs_api.cu", "mcs_api.o", [])]
 
 

@@ -655,8 +655,15 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
-  // multi-warp bisection for plain solves (0: 8 warps, narrowed where rings do not fit)
-  const int coop = sur ? 1 : (o->coop_warps == 0 ? kCoopMaxWarpsHost : o->coop_warps);
+  // multi-warp bisection for plain solves.  By default (0) only for batches of at most
+  // kCoopAutoPerSm points per SM: there the slowest points' serial bisections are the whole
+  // call, while a larger batch is bound by its total work, to which the speculative trials
+  // add (the 4096-speed sweep measured 200 ms with it against 194 ms without).
+  constexpr int kCoopAutoPerSm = 4;
+  const bool coop_auto = n_points <= (size_t)kCoopAutoPerSm * ctx->sms;
+  const int coop = sur ? 1
+                   : o->coop_warps == 0 ? (coop_auto ? kCoopMaxWarpsHost : 1)
+                                        : o->coop_warps;
   rc = make_buckets(ctx, smem, cost, slots, modes, nls, grps, false, o->precision == MCS_FP64,
                     o->max_buckets, order,
                     pl->buckets, &pp, coop);

@@ -127,6 +127,42 @@ class Spindle(C.Structure):
                 ("z_tool", C.c_double), ("z_sp", C.c_double)]
 
 
+END_BINS, END_RINGS, MAX_SLICES = 36, 6, 64
+ENGINE_HIST, ENGINE_TS = 4096, 64
+
+
+class EngineConfig(C.Structure):
+    _fields_ = [("tool", Tool), ("modal", Modal)] + [
+        (n, C.c_double) for n in ("Ktc", "Krc", "Kac", "Kte", "Kre", "Kae", "mc", "Ci", "S",
+                                  "fn_max")] + [("nonlinear", C.c_int32), ("decim", C.c_int32)]
+
+
+class Engagement(C.Structure):
+    _fields_ = [("Hb", C.c_float * 180), ("ux", C.c_double), ("uy", C.c_double),
+                ("fz", C.c_double), ("tip_z", C.c_double), ("ap", C.c_double),
+                ("profile", C.c_int32), ("wear", C.c_int32), ("Kte", C.c_double),
+                ("Kre", C.c_double), ("slice_r", C.c_double * MAX_SLICES),
+                ("slice_kap", C.c_double * MAX_SLICES),
+                ("Eb", C.c_float * (END_BINS * END_RINGS)), ("fza", C.c_double),
+                ("end_r", C.c_double), ("ring_z", C.c_double * END_RINGS),
+                ("ring_zo", C.c_double * END_RINGS), ("ring_zi", C.c_double * END_RINGS),
+                ("wall_k", C.c_double), ("wall_m", C.c_double), ("wall_zeta", C.c_double),
+                ("wall_nx", C.c_double), ("wall_ny", C.c_double)]
+
+
+ENGINE_STATS_FIELDS = ("n", "sumF", "maxF", "sumFx", "sumFy", "sumFz", "maxFz", "sumT",
+                       "maxT", "sumX", "sumY", "minX", "maxX", "minY", "maxY", "sumZc", "wZc",
+                       "sumW", "maxW", "sumHb", "sumB", "sumRb", "engTeeth")
+ENGINE_STATS_DTYPE = np.dtype([(n, "<f8") for n in ENGINE_STATS_FIELDS])
+
+
+class EngineState(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("x", "y", "vx", "vy", "t", "w", "wv", "dt",
+                                          "run_mean_w")] + [
+        (n, C.c_int32) for n in ("pr", "nz", "steps_per_tooth", "steps_per_rev", "max_slices",
+                                 "decim")] + [("step_count", C.c_uint64)]
+
+
 class Peaks(C.Structure):
     _fields_ = [("fp32_tflops", C.c_double), ("fp64_tflops", C.c_double),
                 ("smem_tbps", C.c_double)]

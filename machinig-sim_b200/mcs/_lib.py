@@ -29,6 +29,9 @@ EXPORTS = (
     "mcs_surrogate_get_params", "mcs_surrogate_set_params", "mcs_solve_guided",
     "mcs_plan_create_guided", "mcs_plan_guide_info", "mcs_tune", "mcs_measure_peaks",
     "mcs_modes_at", "mcs_lobes_composite", "mcs_curve_alim", "mcs_solve_multi", "mcs_shard",
+    "mcs_engine_create", "mcs_engine_destroy", "mcs_engine_configure", "mcs_engine_set_engagement",
+    "mcs_engine_set_state", "mcs_engine_run", "mcs_engine_take_stats", "mcs_engine_get_state",
+    "mcs_engine_history", "mcs_engine_reset_history", "mcs_engine_chatter_index",
 )
 _VOID = ("mcs_default_opts", "mcs_last_error", "mcs_stream", "mcs_job_free",
          "mcs_default_train_opts", "mcs_default_guide_opts")
@@ -105,6 +108,13 @@ def load(path: Path | str | None = None):
         L.mcs_curve_alim.argtypes = [vp, vp, C.c_size_t, vp, C.c_size_t, vp]
         L.mcs_solve_multi.argtypes = [vp, C.c_size_t] + batch[1:] + [vp]
         L.mcs_shard.argtypes = batch[1:] + [C.c_size_t, vp, vp]
+        L.mcs_engine_create.argtypes = [vp, C.c_size_t, P(vp)]
+        for f in ("destroy", "reset_history"):
+            getattr(L, f"mcs_engine_{f}").argtypes = [vp]
+        for f in ("configure", "set_engagement", "set_state", "run", "take_stats", "get_state",
+                  "chatter_index"):
+            getattr(L, f"mcs_engine_{f}").argtypes = [vp, vp]
+        L.mcs_engine_history.argtypes = [vp, vp, vp, vp]
         for name in EXPORTS:
             if name not in _VOID:
                 getattr(L, name).restype = C.c_int

@@ -13,6 +13,8 @@
 namespace {
 
 constexpr int kBins = 180;          // cutting.js:15
+constexpr int kEndBins = 36;        // cutting.js:16
+constexpr int kEndRings = 6;        // cutting.js:17
 constexpr double kHRef = 0.05;      // cutting.js:18
 constexpr double kHMin = 0.002;     // cutting.js:19
 constexpr double kPi = 3.141592653589793;
@@ -56,8 +58,17 @@ struct or_engine {
   double x = 0, y = 0, vx = 0, vy = 0, t = 0;
   double x0 = 0, y0 = 0, vx0 = 0, vy0 = 0;
   long long stepCount = 0;
-  // material
-  double Ktc = 0, Krc = 0, Kte = 0, Kre = 0, mc = 0, Ci = 0;
+  // material (Kac, Kae: the axial force; wear: setWear's edge coefficients)
+  double Ktc = 0, Krc = 0, Kte = 0, Kre = 0, mc = 0, Ci = 0, Kac = 0, Kae = 0;
+  bool wear = false;
+  double KteW = 0, KreW = 0;
+  // end edges (setEndEngagement, cutting.js:130-143)
+  float Eb[kEndBins * kEndRings];
+  double fza = 0, endR = 0;
+  double ringR[kEndRings] = {}, ringCos[kEndRings] = {}, ringDs[kEndRings] = {},
+         ringZ[kEndRings] = {};
+  // thin wall (setWork, cutting.js:88-94)
+  double wk = 0, wm = 1, wc = 0, wnx = 1, wny = 0, w = 0, wv = 0, runMeanW = 0;
   // engagement
   float Hb[kBins];
   double ux = 1, uy = 0, vxd = 0, vyd = 1, fz = 0, tipZ = 0, db = 0;
@@ -65,16 +76,26 @@ struct or_engine {
   std::vector<double> sliceB, sliceZ, sliceLag, sliceR, sliceKap;
   // samples and statistics
   SampleRing hist, ts;
-  or_stats st;
+  std::vector<float> histF[3];  // Fx, Fy, Fz of the history ring
+  mcs_engine_stats st;
   std::vector<unsigned char> toothEngaged;
   std::vector<double> toothVol;
   std::vector<double> chipVols;
 
   or_engine() {
     std::memset(Hb, 0, sizeof(Hb));
+    std::memset(Eb, 0, sizeof(Eb));
     hist.reset(4096);
+    for (auto& f : histF) f.assign(4096, 0.f);
     ts.reset(64);
-    std::memset(&st, 0, sizeof(st));
+    new_stats(st);
+  }
+  static void new_stats(mcs_engine_stats& s) {  // newStats() (cutting.js:324-327)
+    std::memset(&s, 0, sizeof(s));
+    s.minX = INFINITY;
+    s.maxX = -INFINITY;
+    s.minY = INFINITY;
+    s.maxY = -INFINITY;
   }
 };
 
@@ -148,10 +169,32 @@ void or_engine_configure(or_engine* e, const mcs_tool* tool, int nonlinear,
   e->Kre = mat->Kre;
   e->mc = mat->mc;
   e->Ci = mat->Ci;
+  // setWork(null) and no end-edge feed (cutting.js:73-75)
+  e->wk = 0;
+  e->wm = 1;
+  e->wc = 0;
+  e->w = 0;
+  e->wv = 0;
+  e->wnx = 1;
+  e->wny = 0;
+  e->runMeanW = 0;
+  e->fza = 0;
 }
+
+void or_engine_set_engagement_profile(or_engine* e, double ux, double uy, double fz,
+                                      double tipZ, double ap, const double* prof_r,
+                                      const double* prof_kap);
 
 void or_engine_set_engagement(or_engine* e, double ux, double uy, double fz, double tipZ,
                               double ap) {
+  or_engine_set_engagement_profile(e, ux, uy, fz, tipZ, ap, nullptr, nullptr);
+}
+
+// setEngagement with a general edge profile: slice k's radius prof_r[k] and kappa
+// prof_kap[k], as rAt gives them (cutting.js:115-118); NULL: the flat / ball rule
+void or_engine_set_engagement_profile(or_engine* e, double ux, double uy, double fz,
+                                      double tipZ, double ap, const double* prof_r,
+                                      const double* prof_kap) {
   e->ux = ux;
   e->uy = uy;
   e->vxd = -uy;
@@ -181,7 +224,10 @@ void or_engine_set_engagement(or_engine* e, double ux, double uy, double fz, dou
     const double zr = k * e->dz + 0.5 * e->sliceB[k];
     e->sliceZ[k] = tipZ + zr;
     double r = R, kap = 1;
-    if (e->type == MCS_TOOL_BALL && zr < R) {
+    if (prof_r) {
+      r = prof_r[k];
+      kap = prof_kap[k];
+    } else if (e->type == MCS_TOOL_BALL && zr < R) {
       const double d = R - zr;
       r = std::sqrt(std::max(1e-6, R * R - d * d));
       kap = r / R;
@@ -203,7 +249,9 @@ void or_engine_run(or_engine* e, int64_t nSteps) {
   const int N = e->N, spt = e->spt, spr = e->spr, nz = e->nz;
   float* surf = e->surf.data();
   const double ux = e->ux, uy = e->uy, vx = e->vxd, vy = e->vyd, fz = e->fz, dt = e->dt;
-  const double Ktc = e->Ktc, Krc = e->Krc, Kte = e->Kte, Kre = e->Kre;
+  const double Ktc = e->Ktc, Krc = e->Krc, Kac = e->Kac, Kae = e->Kae;
+  // edge coefficients grow with the flank wear land (setWear)
+  const double Kte = e->wear ? e->KteW : e->Kte, Kre = e->wear ? e->KreW : e->Kre;
   const bool nl = e->nonlinear;
   const double mc = nl ? e->mc : 0;
   // process damping per slice [N s/m] = Ci b / V_c (cutting.js:155-156)
@@ -211,6 +259,8 @@ void or_engine_run(or_engine* e, int64_t nSteps) {
   const double TWO_PI = 2 * kPi, binScale = kBins / TWO_PI, pitch = TWO_PI / N;
   const double dphi = e->omega * dt;
   const double hMax = std::max(0.1, 3 * fz);
+  const float* Eb = e->Eb;
+  const double fza = e->fza;
   ModeBank& MX = e->mx;
   ModeBank& MY = e->my;
   const int nmx = (int)MX.k.size(), nmy = (int)MY.k.size();
@@ -221,14 +271,19 @@ void or_engine_run(or_engine* e, int64_t nSteps) {
   MY.v[0] += e->vy - e->vy0;
   double x = e->x, y = e->y, vxs = e->vx, vys = e->vy, t = e->t;
   int pr = e->pr;
-  or_stats& st = e->st;
+  const double wk = e->wk, wm = e->wm, wc = e->wc, wnx = e->wnx, wny = e->wny;
+  double w = e->w, wv = e->wv, wSum = 0;
+  mcs_engine_stats& st = e->st;
   SampleRing& hist = e->hist;
   SampleRing& ts = e->ts;
   for (int64_t s = 0; s < nSteps; s++) {
     const double theta = pr * dphi;
-    const double xm = x * 1e3, ym = y * 1e3;  // rigid workpiece: w = 0
-    double Fx = 0, Fy = 0;
-    const double rvx = vxs, rvy = vys;
+    // tool position relative to the (possibly deflected) workpiece [mm]
+    const double rx = x - w * wnx, ry = y - w * wny;
+    const double xm = rx * 1e3, ym = ry * 1e3;
+    double Fx = 0, Fy = 0, Fz = 0, T = 0, Fr2z = 0, Fsum = 0;
+    // relative tool-to-wall velocity [m/s] for process damping
+    const double rvx = vxs - wv * wnx, rvy = vys - wv * wny;
     for (int i = 0; i < N; i++) {
       int engaged = 0;
       const double dRi = e->dR[i];
@@ -264,12 +319,49 @@ void or_engine_run(or_engine* e, int64_t nSteps) {
         const double bk = e->sliceB[k];
         const double Ft = Ktc * se * h * bk + Kte * bk;
         double Fr = Krc * se * h * bk + Kre * bk;
+        const double Fa = Kac * se * h * bk + Kae * bk;
         if (pdK != 0) Fr += pdK * (bk / e->db) / e->sliceR[k] * (rvx * nxg + rvy * nyg);
         const double txg = cs * ux - sn * vx, tyg = cs * uy - sn * vy;
         Fx += -Ft * txg - Fr * nxg;
         Fy += -Ft * tyg - Fr * nyg;
+        Fz -= Fa;
+        T += Ft * e->sliceR[k];
+        const double fr = std::hypot(Ft, Fr);
+        Fsum += fr;
+        Fr2z += fr * (e->sliceZ[k] - e->tipZ);
         engaged = 1;
+        st.sumHb += h * bk;
+        st.sumB += bk;
+        st.sumRb += e->sliceR[k] * h * bk;
         e->toothVol[i] += h * bk * e->sliceR[k] * dphi;
+      }
+      if (fza != 0) {
+        // end edges at the tip (no helix lag): thrust, torque, in-plane tangential force
+        double phi = std::fmod(theta + i * pitch, TWO_PI);
+        if (phi < 0) phi += TWO_PI;
+        const int row = ((int)(phi / TWO_PI * kEndBins)) * kEndRings;
+        const double sn = std::sin(phi), cs = std::cos(phi);
+        const double txg = cs * ux - sn * vx, tyg = cs * uy - sn * vy;
+        for (int j = 0; j < kEndRings; j++) {
+          const double depth = row < kEndBins * kEndRings ? (double)Eb[row + j] : 0.0;
+          if (depth <= 2e-4) continue;
+          const double c = e->ringCos[j], ds = e->ringDs[j];
+          const double h = (depth < fza ? depth : fza) * c;
+          const double se = mc != 0 ? std::pow(kHRef / (h > kHMin ? h : kHMin), mc) : 1;
+          const double Ft = Ktc * se * h * ds + Kte * ds;
+          const double Fn = Krc * se * h * ds + Kre * ds;
+          Fx += -Ft * txg;
+          Fy += -Ft * tyg;
+          Fz -= Fn * c;
+          T += Ft * e->ringR[j];
+          Fsum += Ft;
+          Fr2z += Ft * e->ringZ[j];
+          engaged = 1;
+          st.sumHb += h * ds;
+          st.sumB += ds;
+          st.sumRb += e->ringR[j] * h * ds;
+          e->toothVol[i] += h * ds * e->ringR[j] * dphi;
+        }
       }
       if (!engaged && e->toothEngaged[i]) {
         if (e->toothVol[i] > 0) e->chipVols.push_back(e->toothVol[i]);
@@ -295,27 +387,60 @@ void or_engine_run(or_engine* e, int64_t nSteps) {
       y += MY.q[j];
       vys += MY.v[j];
     }
+    if (wk != 0) {
+      // reaction on the wall: opposite to the force on the tool, along the wall normal
+      const double Fw = -(Fx * wnx + Fy * wny);
+      wv += (Fw - wc * wv - wk * w) / wm * dt;
+      w += wv * dt;
+      // the wall cannot be pushed further than the material the cutter is engaged in
+      if (w > 5e-4) {
+        w = 5e-4;
+        if (wv > 0) wv = 0;
+      } else if (w < -2e-4) {
+        w = -2e-4;
+        if (wv < 0) wv = 0;
+      }
+      st.sumW += w;
+      st.maxW = std::max(st.maxW, std::fabs(w));
+      wSum += w;
+    }
     if (++pr == spr) pr = 0;
     const int ph = pr % spt;
     if (ph == 0) {  // once-per-tooth sample (:266-268)
-      ts.x[ts.i] = (float)x;
-      ts.y[ts.i] = (float)y;
+      ts.x[ts.i] = (float)(x - w * wnx);
+      ts.y[ts.i] = (float)(y - w * wny);
       ts.i = (ts.i + 1) % ts.n;
       ts.count++;
     }
     t += dt;
+    // statistics (:280-287)
     const double Fxy = std::hypot(Fx, Fy);
     st.n++;
     st.sumF += Fxy;
     st.maxF = std::max(st.maxF, Fxy);
     st.sumFx += Fx;
     st.sumFy += Fy;
+    st.sumFz += Fz;
+    st.maxFz = std::max(st.maxFz, -Fz);
+    st.sumT += T;
+    st.maxT = std::max(st.maxT, T);
     st.sumX += x;
     st.sumY += y;
+    st.minX = std::min(st.minX, x);
+    st.maxX = std::max(st.maxX, x);
+    st.minY = std::min(st.minY, y);
+    st.maxY = std::max(st.maxY, y);
+    if (Fsum > 0) {
+      st.sumZc += Fr2z / Fsum * Fxy;
+      st.wZc += Fxy;
+    }
     if (++e->stepCount % e->decim == 0) {  // decimated history (:288-292)
       const int j = hist.i;
-      hist.x[j] = (float)(x * 1e6);
-      hist.y[j] = (float)(y * 1e6);
+      e->histF[0][j] = (float)Fx;
+      e->histF[1][j] = (float)Fy;
+      e->histF[2][j] = (float)Fz;
+      hist.x[j] = (float)((x - w * wnx) * 1e6);
+      hist.y[j] = (float)((y - w * wny) * 1e6);
       hist.i = (j + 1) % hist.n;
       hist.count++;
     }
@@ -326,6 +451,87 @@ void or_engine_run(or_engine* e, int64_t nSteps) {
   e->vy = e->vy0 = vys;
   e->t = t;
   e->pr = pr;
+  e->w = w;
+  e->wv = wv;
+  e->runMeanW = nSteps ? wSum / nSteps : 0;  // mean wall deflection over this call [m]
+}
+
+void or_engine_set_axial(or_engine* e, double Kac, double Kae) {
+  e->Kac = Kac;
+  e->Kae = Kae;
+}
+
+void or_engine_set_wear(or_engine* e, int on, double Kte, double Kre) {
+  e->wear = on != 0;
+  e->KteW = Kte;
+  e->KreW = Kre;
+}
+
+float* or_engine_eb(or_engine* e) { return e->Eb; }
+
+// setEndEngagement(fza, rOut, zAt) (cutting.js:130-143) with zAt sampled by the caller at
+// each ring radius r_j and at min(rOut, r_j + dr/4), max(0, r_j - dr/4)
+void or_engine_set_end(or_engine* e, double fza, double rOut, const double* z_at,
+                       const double* z_out, const double* z_in) {
+  e->fza = fza > 0 ? fza : 0;
+  e->endR = rOut;
+  const double dr = rOut / kEndRings;
+  for (int j = 0; j < kEndRings; j++) {
+    const double r = (j + 0.5) * dr;
+    const double slope = (z_out[j] - z_in[j]) / (0.5 * dr);
+    const double c = std::max(0.22, 1 / std::sqrt(1 + slope * slope));
+    e->ringR[j] = r;
+    e->ringCos[j] = c;
+    e->ringDs[j] = dr / c;
+    e->ringZ[j] = z_at[j];
+  }
+}
+
+// setWork(wall) (cutting.js:88-94); k <= 0 is setWork(null)
+void or_engine_set_work(or_engine* e, double k, double m, double zeta, double nx, double ny) {
+  if (!(k > 0)) {
+    e->runMeanW = 0;
+    e->wk = 0;
+    e->wm = 1;
+    e->wc = 0;
+    e->w = 0;
+    e->wv = 0;
+    e->wnx = 1;
+    e->wny = 0;
+    return;
+  }
+  // carry the wall state over only while the normal stays roughly the same
+  if (e->wk != 0 && nx * e->wnx + ny * e->wny < 0.8) {
+    e->w = 0;
+    e->wv = 0;
+  }
+  e->wk = k * 1e3;
+  e->wm = m;
+  e->wc = 2 * zeta * std::sqrt(e->wk * m);
+  e->wnx = nx;
+  e->wny = ny;
+}
+
+void or_engine_take_stats_full(or_engine* e, mcs_engine_stats* out) {
+  *out = e->st;
+  or_engine::new_stats(e->st);
+}
+
+// the history ring: out[c * 4096 + j] for c = Fx, Fy, Fz, x, y
+void or_engine_history(const or_engine* e, float* out, int32_t* head, int64_t* count) {
+  const int n = e->hist.n;
+  for (int c = 0; c < 3; c++) std::copy(e->histF[c].begin(), e->histF[c].end(), out + c * n);
+  std::copy(e->hist.x.begin(), e->hist.x.end(), out + 3 * n);
+  std::copy(e->hist.y.begin(), e->hist.y.end(), out + 4 * n);
+  *head = e->hist.i;
+  *count = e->hist.count;
+}
+
+void or_engine_set_decim(or_engine* e, int decim) { e->decim = decim > 0 ? decim : e->decim; }
+
+void or_engine_reset_history(or_engine* e) {
+  e->hist.i = 0;
+  e->hist.count = 0;
 }
 
 void or_engine_chatter_index(const or_engine* e, double out[3]) {
@@ -377,8 +583,16 @@ void or_engine_chatter_index(const or_engine* e, double out[3]) {
 }
 
 void or_engine_take_stats(or_engine* e, or_stats* out) {
-  *out = e->st;
-  std::memset(&e->st, 0, sizeof(e->st));
+  const mcs_engine_stats& s = e->st;
+  out->n = s.n;
+  out->sumF = s.sumF;
+  out->maxF = s.maxF;
+  out->sumFx = s.sumFx;
+  out->sumFy = s.sumFy;
+  out->sumX = s.sumX;
+  out->sumY = s.sumY;
+  out->engTeeth = s.engTeeth;
+  or_engine::new_stats(e->st);
 }
 
 int or_engine_chip_vols(const or_engine* e, double* out, int cap) {

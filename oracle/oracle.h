@@ -24,9 +24,11 @@
  * reference is pinned by the known-answer checks its own tests and design notes give
  * (see tests/test_oracle_pins.py), not bit for bit.
  *
- * Parts of CuttingEngine that the stability path never reaches are left out: end-edge
- * forces (fza, cutting.js:130-143,215-237), the thin-wall mode (:88-94,256-264), wall
- * samples (:269-277) and the rAt edge profile (:115-119).
+ * The engine also restates the terms the stability path never reaches, for the playback
+ * and identification checks: the axial force and torque, end-edge forces (fza,
+ * cutting.js:130-143,215-237), the thin-wall mode (:88-94,256-264), a general edge profile
+ * per slice (:115-119), the full statistics and the force history.  Wall samples
+ * (:269-277, roughness only) are left out.
  */
 #ifndef MCS_ORACLE_H_
 #define MCS_ORACLE_H_
@@ -77,6 +79,24 @@ void or_engine_take_stats(or_engine* e, or_stats* out);
 /* Volumes of the chip events so far, oldest first (cutting.js:238-242). */
 int or_engine_chip_vols(const or_engine* e, double* out, int cap);
 void or_engine_get_info(const or_engine* e, or_engine_info* out);
+/* The rest of the engine's cutting terms, for the playback / identification oracle: the
+ * axial coefficients, setWear, the end-face map Eb (36 x 6 floats, filled by callers),
+ * setEndEngagement with the tip profile sampled at the rings, setWork (k <= 0: none), a
+ * general edge profile per slice, the full takeStats() and the force/position history. */
+void or_engine_set_axial(or_engine* e, double Kac, double Kae);
+void or_engine_set_wear(or_engine* e, int on, double Kte, double Kre);
+float* or_engine_eb(or_engine* e);
+void or_engine_set_end(or_engine* e, double fza, double rOut, const double* z_at,
+                       const double* z_out, const double* z_in);
+void or_engine_set_work(or_engine* e, double k, double m, double zeta, double nx, double ny);
+void or_engine_set_engagement_profile(or_engine* e, double ux, double uy, double fz,
+                                      double tipZ, double ap, const double* prof_r,
+                                      const double* prof_kap);
+void or_engine_take_stats_full(or_engine* e, mcs_engine_stats* out);
+void or_engine_history(const or_engine* e, float* out, int32_t* head, int64_t* count);
+void or_engine_reset_history(or_engine* e);
+/* e.decim = decim (validate.js:80 samples every step). */
+void or_engine_set_decim(or_engine* e, int decim);
 
 /* ---- stabtd.js ---- */
 /* One chatterAt trial (stabtd.js:14-22) with the option set of mcs_opts. */

@@ -109,6 +109,18 @@ def lib():
     L.or_sdm_limit.restype = C.c_double
     L.or_tool_model.argtypes = [C.c_double] * 4 + [P(C.c_double)]
     L.or_immersion.argtypes = [C.c_int, C.c_double, C.c_double, P(C.c_double)]
+    L.or_engine_set_axial.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    L.or_engine_set_wear.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+    L.or_engine_eb.restype = P(C.c_float)
+    L.or_engine_eb.argtypes = [C.c_void_p]
+    L.or_engine_set_end.argtypes = [C.c_void_p, C.c_double, C.c_double] + [P(C.c_double)] * 3
+    L.or_engine_set_work.argtypes = [C.c_void_p] + [C.c_double] * 5
+    L.or_engine_set_engagement_profile.argtypes = [C.c_void_p] + [C.c_double] * 5 + [
+        P(C.c_double)] * 2
+    L.or_engine_take_stats_full.argtypes = [C.c_void_p, C.c_void_p]
+    L.or_engine_history.argtypes = [C.c_void_p, C.c_void_p, P(C.c_int32), P(C.c_int64)]
+    L.or_engine_reset_history.argtypes = [C.c_void_p]
+    L.or_engine_set_decim.argtypes = [C.c_void_p, C.c_int]
     L.or_modes_at.argtypes = [P(A.Spindle), C.c_void_p, C.c_size_t, P(C.c_double), C.c_size_t,
                               C.c_void_p]
     L.or_modes_at.restype = None
@@ -185,6 +197,51 @@ class Engine:
         i = EngineInfo()
         self._L.or_engine_get_info(self._h, C.byref(i))
         return {n: getattr(i, n) for n, _ in EngineInfo._fields_}
+
+    # the playback / identification terms, driven by the library's record types
+    def configure_from(self, c: A.EngineConfig):
+        """configure() from an mcs_engine_config record (the same inputs the GPU engine
+        gets), the axial coefficients and the decimation with it."""
+        mat = A.Material(c.Ktc, c.Krc, c.Kte, c.Kre, c.mc, c.Ci)
+        self._L.or_engine_configure(self._h, C.byref(c.tool), int(c.nonlinear),
+                                    C.byref(c.modal), C.byref(mat), c.S, c.fn_max, 0, 0)
+        self._L.or_engine_set_axial(self._h, c.Kac, c.Kae)
+        if c.decim > 0:
+            self._L.or_engine_set_decim(self._h, int(c.decim))
+
+    def engage(self, g: A.Engagement):
+        """setEngagement, setEndEngagement, setWork and setWear from an mcs_engagement."""
+        self.Hb[:] = np.frombuffer(bytes(g.Hb), dtype=np.float32)
+        r = np.frombuffer(bytes(g.slice_r), dtype=np.float64).copy()
+        k = np.frombuffer(bytes(g.slice_kap), dtype=np.float64).copy()
+        if g.profile:
+            self._L.or_engine_set_engagement_profile(self._h, g.ux, g.uy, g.fz, g.tip_z, g.ap,
+                                                     _dptr(r), _dptr(k))
+        else:
+            self.set_engagement((g.ux, g.uy), g.fz, g.tip_z, g.ap)
+        eb = np.ctypeslib.as_array(self._L.or_engine_eb(self._h), shape=(36 * 6,))
+        eb[:] = np.frombuffer(bytes(g.Eb), dtype=np.float32)
+        rz = [np.frombuffer(bytes(a), dtype=np.float64).copy() for a in (g.ring_z, g.ring_zo,
+                                                                          g.ring_zi)]
+        self._L.or_engine_set_end(self._h, g.fza, g.end_r, *[_dptr(a) for a in rz])
+        self._L.or_engine_set_work(self._h, g.wall_k, g.wall_m, g.wall_zeta, g.wall_nx,
+                                   g.wall_ny)
+        self._L.or_engine_set_wear(self._h, int(g.wear), g.Kte, g.Kre)
+
+    def take_stats_full(self) -> np.ndarray:
+        out = np.zeros(1, dtype=A.ENGINE_STATS_DTYPE)
+        self._L.or_engine_take_stats_full(self._h, C.c_void_p(out.ctypes.data))
+        return out[0]
+
+    def history(self):
+        out = np.zeros((5, A.ENGINE_HIST), dtype=np.float32)
+        head, count = C.c_int32(), C.c_int64()
+        self._L.or_engine_history(self._h, C.c_void_p(out.ctypes.data), C.byref(head),
+                                  C.byref(count))
+        return out, head.value, count.value
+
+    def reset_history(self):
+        self._L.or_engine_reset_history(self._h)
 
 
 # ---------------------------------------------------------------- stabtd.js
