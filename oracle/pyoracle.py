@@ -431,3 +431,47 @@ def composite_lobes(spindle: A.Spindle, params: dict, frfs=()):
             S += LOBE_STEP
         S0 += LOBE_NODE
     return [curve]
+
+
+# ---------------------------------------------------------------- identify.js / validate.js
+def _rigid_engine(cfg, g):
+    e = Engine()
+    e.configure_from(cfg)
+    e.engage(g)
+    return e
+
+
+def unit_forces_ref(cfgs, gs):
+    """unitForces (src/identify.js:26-40) per prepared (config, engagement) pair: two
+    revolutions, takeStats, one revolution; the mean force on the workpiece (-sum/n)."""
+    out = []
+    for c, g in zip(cfgs, gs):
+        e = _rigid_engine(c, g)
+        spr = e.info()["steps_per_rev"]
+        e.run(2 * spr)
+        e.take_stats_full()
+        e.run(spr)
+        s = e.take_stats_full()
+        out.append([-s["sumFx"] / s["n"], -s["sumFy"] / s["n"], -s["sumFz"] / s["n"]])
+    return np.array(out)
+
+
+def sim_revolution_ref(cfg, g, nb=360):
+    """simRevolution (src/validate.js:76-100) for a prepared (config, engagement) pair whose
+    config samples every step: two revolutions, the history emptied, one revolution, then
+    the history interpolated onto nb angle bins (force on the workpiece)."""
+    e = _rigid_engine(cfg, g)
+    n = e.info()["steps_per_rev"]
+    e.run(2 * n)
+    e.reset_history()
+    e.run(n)
+    h, _, _ = e.history()
+    out = np.zeros((3, nb))
+    for c in range(3):
+        for b in range(nb):
+            x = (b + 0.5) / nb * n - 0.5
+            i0 = math.floor(x)
+            f = x - i0
+            a, cc = float(h[c][(i0 + n) % n]), float(h[c][(i0 + 1) % n])
+            out[c][b] = -(a + (cc - a) * f)
+    return out
