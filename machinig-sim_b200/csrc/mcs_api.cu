@@ -389,8 +389,9 @@ namespace {
 // Multi-warp bisection: the heaviest buckets of a plain solve, as long as their points
 // together number at most one per SM, run each point on `coop` warps of one block (the
 // latency tail of the slowest points; see solve_coop_kernel).  Buckets whose points pack
-// trials into lane groups keep them: that speculation needs no extra warps.  pp (NULL for
-// trial batches) gives the per-point sizes the multi-warp shared memory follows from.
+// trials into lane groups keep them while their deepest trials fit in half a warp: that
+// speculation needs no extra warps.  pp (NULL for trial batches) gives the per-point sizes
+// the multi-warp shared memory follows from.
 int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
                  const std::vector<int>& slots, const std::vector<int>& modes,
                  const std::vector<int>& nls, const std::vector<int>& grps, bool trials,
@@ -438,7 +439,14 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     b.smem = (top + 15) & ~15;
     b.shape = KernelShape{sl, nm, fp64, nl, trials ? 0 : gr};
     order.insert(order.end(), seg.begin(), seg.end());
-    if (!trials && pp && coop_warps > 1 && gr == 0 && (int)order.size() <= ctx->sms) {
+    // lane groups speculate without extra warps, but only while a trial's slices fit in a
+    // fraction of the warp: points whose deepest trials need more than half of it run
+    // their deep levels serially there, and take the multi-warp path like the others
+    int nz_top = 0;
+    if (pp)
+      for (int32_t q : seg) nz_top = std::max(nz_top, (*pp)[q].nz_max);
+    if (!trials && pp && coop_warps > 1 && (gr == 0 || nz_top > kWarp / 2) &&
+        (int)order.size() <= ctx->sms) {
       // the widest block whose rings fit: the requested width, else 4, else 3
       for (int wv : {coop_warps, 4, 3}) {
         if (wv > coop_warps) continue;
@@ -757,7 +765,7 @@ void mcs_default_opts(mcs_opts* o) {
   o->steps_per_tooth = 0;
   o->slices = 0;
   o->chatter_idx = 0.45;
-  o->precision = MCS_FP32;
+  o->precision = MCS_FP64;  // the reference's arithmetic; MCS_FP32 is the faster variant
   o->max_buckets = 0;
   o->serial_trials = 0;
   o->coop_warps = 0;

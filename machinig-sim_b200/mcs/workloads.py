@@ -187,7 +187,10 @@ def hetero_setups(seeds: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray
     return st, md, speed
 
 
-HETERO_OPTS = dict(aMin=0.05, aMax=15.0, iters=10, revs=60, nonlinear=True, honorRunout=True)
+# the heterogeneous batches run FP32 integration: the surrogate's labels are FP32 limits and
+# guided serving is compared with the plain FP32 bisection
+HETERO_OPTS = dict(aMin=0.05, aMax=15.0, iters=10, revs=60, nonlinear=True, honorRunout=True,
+                   precision="fp32")
 
 
 def hetero(n: int = 16384, first_seed: int = 0) -> Workload:

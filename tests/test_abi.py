@@ -159,7 +159,8 @@ def test_tool_conversion_units():
 def test_precision_option():
     from mcs import _abi as A
 
-    assert A.make_opts().precision == A.FP32
+    assert A.make_opts().precision == A.FP64  # the reference's arithmetic by default
+    assert A.make_opts(precision="fp32").precision == A.FP32
     assert A.make_opts(precision="fp64").precision == A.FP64
     with pytest.raises(ValueError):
         A.make_opts(precision="fp16")
