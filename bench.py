@@ -52,6 +52,8 @@ WORKLOADS = {
     "hetero": "hetero: 16384 seeded setups (D 3-20 mm, 2-6 flutes, helix 0-45, runout 0-20 um, "
               "1-3 modes per axis, process damping and size effect), [0.05,15] x 10, 60 revs, "
               "reference slice rule",
+    "small": "small: 64 speeds 5000-20000 rpm, 4-flute D10 helix 30, 1 mode per axis, no "
+             "runout, linear, [0.1,10] x 10, 60 revs, 200 steps per tooth, 40 slices",
 }
 METRIC = "stability-boundary points/sec on 1 B200: surrogate-guided vs plain GPU vs Node CPU @<=2% depth err"
 UNIT = "points/s"
@@ -195,9 +197,12 @@ def run_oracle(wl, idx, threads: int):
 
 
 def fp64_subset(wl) -> np.ndarray:
-    """The workload's seeded 256-point subset (the golden fixtures hold the same points)."""
+    """The workload's seeded 256-point subset (the golden fixtures hold the same points);
+    a workload of at most 256 points is its own subset."""
     from mcs import workloads as W
 
+    if wl.n <= 256:
+        return np.arange(wl.n)
     if "fp64_subset" in wl.meta:
         return np.asarray(wl.meta["fp64_subset"])
     return np.sort(np.argsort(W.uniform(np.arange(wl.n), 7, 0))[:256])
@@ -422,6 +427,8 @@ def make_workload(name: str, rank: int, points: int = 0):
 
     if name == "hetero":  # 16384 seeded setups per rank (weak scaling)
         wl = W.hetero(n=16384, first_seed=16384 * rank)
+    elif name == "small":  # the 64-speed reference case; the same on every rank
+        wl = W.small()
     else:
         wl = W.sweep(seed=1 + rank)
     if points and points < wl.n:  # a smaller case of the same workload (profiling)
@@ -622,10 +629,13 @@ def ours(args) -> int:
                                 [p for p in ("fp64", "fp32") if p != args.precision])
     main = measure(args.workload, precs, args.steps, args.warmup,
                    0 if args.no_e2e else max(2, min(args.steps, 5)), not args.no_cpu)
-    hetero = None
+    hetero = small = None
     if not args.no_hetero and args.workload != "hetero":
         hetero = measure("hetero", precs, max(3, min(args.steps, 5)), 3,
                          0 if args.no_e2e else 2, not args.no_cpu)
+    if not args.no_small and args.workload != "small":
+        small = measure("small", precs, max(3, min(args.steps, 5)), 3,
+                        0 if args.no_e2e else 2, not args.no_cpu)
 
     if rank == 0:
         head = summarize(args.workload, main, args.precision)
@@ -654,8 +664,10 @@ def ours(args) -> int:
             "results": {"open": int(v["res"]["open"].sum()),
                         "alim_median": float(np.median(v["res"]["alim"]))},
             "variants": head["variants"],
-            "workloads": {"hetero": summarize("hetero", hetero, args.precision)}
-            if hetero else None,
+            "workloads": {**({"hetero": summarize("hetero", hetero, args.precision)}
+                             if hetero else {}),
+                          **({"small": summarize("small", small, args.precision)}
+                             if small else {})} or None,
             "guided": guided,
             "worker_latency": latency,
         }
@@ -684,11 +696,12 @@ def main(argv=None) -> int:
     ap.add_argument("--no-guided", action="store_true",
                     help="skip the surrogate-guided serving leg")
     ap.add_argument("--no-hetero", action="store_true", help="skip the hetero workload leg")
+    ap.add_argument("--no-small", action="store_true", help="skip the 64-speed reference case")
     ap.add_argument("--guided-repeats", type=int, default=5)
     ap.add_argument("--no-latency", action="store_true",
                     help="skip the latency of the Worker's 18-speed request")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "hetero"],
-                    help="sweep (the headline) or the heterogeneous batch")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "hetero", "small"],
+                    help="sweep (the headline), the heterogeneous batch or the 64-speed case")
     ap.add_argument("--max-buckets", type=int, default=0,
                     help="fixed schedule (shared-memory size classes); 0: autotune")
     ap.add_argument("--coop-warps", type=int, default=-1,
