@@ -528,12 +528,15 @@ def ours(args) -> int:
         """Device-resident plan of a workload: per-step CUDA-event times, results, info."""
         opts = A.make_opts(precision=precision)
         for f in ("a_min", "a_max", "iters", "revs", "nonlinear", "honor_runout",
-                  "steps_per_tooth", "slices", "chatter_idx", "serial_trials", "coop_warps"):
+                  "steps_per_tooth", "slices", "chatter_idx", "serial_trials", "coop_warps",
+                  "coop_points"):
             setattr(opts, f, getattr(wl.opts, f))
         if args.serial_trials:
             opts.serial_trials = 1
         if args.coop_warps >= 0:
             opts.coop_warps = args.coop_warps
+        if args.coop_points >= 0:
+            opts.coop_points = args.coop_points
         # schedule (number of shared-memory size classes) from the autotuner, untimed
         if args.max_buckets:
             opts.max_buckets, tuned = args.max_buckets, {"ms": {}, "cached": False}
@@ -545,6 +548,7 @@ def ours(args) -> int:
         info["schedule"] = {"max_buckets": int(opts.max_buckets), "tuning_ms": tuned["ms"],
                             "from_cache": bool(tuned["cached"]),
                             "coop_warps": int(opts.coop_warps),
+                            "coop_points_opt": int(opts.coop_points),
                             "coop_points": int(info["coop_points"])}
         for _ in range(warmup):
             plan.execute()
@@ -706,6 +710,9 @@ def main(argv=None) -> int:
                     help="fixed schedule (shared-memory size classes); 0: autotune")
     ap.add_argument("--coop-warps", type=int, default=-1,
                     help="warps sharing each heaviest point's bisection (1: off; -1: default)")
+    ap.add_argument("--coop-points", type=int, default=-1,
+                    help="how many of the costliest points take that path (0: one per SM; "
+                         "-1: default)")
     ap.add_argument("--strong", action="store_true",
                     help="N > 1: split one batch over the ranks (mcs_shard) instead of one "
                          "batch per rank")

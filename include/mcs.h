@@ -119,19 +119,30 @@ typedef struct {
   double chatter_idx;      /* decision threshold (reference 0.45, stabtd.js:10) */
   int32_t precision;       /* mcs_precision of the force law and modal integration */
   int32_t max_buckets;     /* schedule: at most this many shared-memory size classes, each
-                              its own persistent grid (1..MCS_MAX_BUCKETS; 0: 16); results
-                              do not depend on it, only the time does (see mcs_tune) */
+                              its own persistent grid (1..MCS_MAX_BUCKETS; 0: 16), besides
+                              one grid per block width of the multi-warp points (coop_warps);
+                              results do not depend on it, only the time does (see
+                              mcs_tune) */
   int32_t serial_trials;   /* 0: a bisection runs the trials of its next levels together in
                               lane groups of one warp when their slice counts allow
                               (speculatively; only the trials on the decision path count);
                               1: one trial at a time.  Results are identical either way. */
-  int32_t coop_warps;      /* schedule: the heaviest points (up to one per SM) share their
-                              bisection among this many warps of one block, each running one
-                              trial of the next levels speculatively (2..8, narrowed to 4 or 3
-                              where the rings do not fit in shared memory; 1: off; 0: 8 for
-                              batches of at most 4 points per SM, where the slowest points'
-                              serial bisections are the whole call, else off).  Plain solves
-                              only.  Results are identical either way. */
+  int32_t coop_warps;      /* schedule: the heaviest points share their bisection among this
+                              many warps of one block, each running one trial of the next
+                              levels speculatively (2..8, narrowed to 4 or 3 where the rings
+                              do not fit in shared memory; 1: off; 0: the library's rule,
+                              see coop_points).  Plain solves only.  Results are identical
+                              either way. */
+  int32_t coop_points;     /* schedule: how many of the costliest points take that path
+                              (0: one per SM).  With coop_warps and coop_points both 0 the
+                              library's rule applies: 8 warps (or the widest that fits) for
+                              each point whose serial bisection costs more than the batch's
+                              share of one resident warp -- the points that would still run
+                              once the device has done the rest -- up to two per SM; none
+                              in a batch bound by its total work.  Points whose trials
+                              share a warp in lane groups (all of them in at most half a
+                              warp) keep that instead. */
+  int32_t pad;
 } mcs_opts;
 
 #define MCS_MAX_BUCKETS 32

@@ -76,6 +76,7 @@ int check_inputs(const mcs_setup* setups, size_t n_setups, const mcs_modal* moda
     return fail(MCS_ERR_ARG, "serial_trials must be 0 or 1");
   if (o->coop_warps < 0 || o->coop_warps > kCoopMaxWarpsHost)
     return fail(MCS_ERR_ARG, "coop_warps out of range [0, %d]", kCoopMaxWarpsHost);
+  if (o->coop_points < 0) return fail(MCS_ERR_ARG, "coop_points must be >= 0");
   for (size_t i = 0; i < n_setups; i++) {
     const mcs_setup& s = setups[i];
     const mcs_tool& t = s.tool;
@@ -383,31 +384,150 @@ struct mcs_job {
 
 namespace {
 
+// The multi-warp head of a plain solve: the `head` costliest points (in cost order) that
+// do not speculate in lane groups already, each on the widest block whose rings fit in
+// shared memory (`coop_warps`, else 4, else 3 warps; a point that fits none stays on the
+// one-warp path).  One bucket per width, the one holding the costliest point first; the
+// points of all of them are appended to `members` in bucket order.
+void coop_head_buckets(const std::vector<double>& cost, const std::vector<int>& slots,
+                       const std::vector<int>& modes, const std::vector<int>& nls,
+                       const std::vector<int>& grps, const std::vector<PointParams>& pp,
+                       int fp64, int coop_warps, int head, std::vector<int32_t>& members,
+                       std::vector<Bucket>& heads) {
+  const size_t n = cost.size();
+  std::vector<int32_t> byc(n);
+  std::iota(byc.begin(), byc.end(), 0);
+  std::stable_sort(byc.begin(), byc.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+  members.clear();
+  heads.clear();
+  const int widths[3] = {coop_warps, std::min(coop_warps, 4), std::min(coop_warps, 3)};
+  std::vector<int32_t> part[3];
+  int taken = 0;
+  for (int32_t q : byc) {
+    if (taken >= head) break;
+    // lane groups speculate without extra warps, but only while a trial's slices fit in a
+    // fraction of the warp: points whose deepest trials need more than half of it run
+    // their deep levels serially there, and take the multi-warp path like the others
+    if (grps[q] && pp[q].nz_max <= kWarp / 2) continue;
+    for (int k = 0; k < 3; k++) {
+      if (k > 0 && widths[k] == widths[k - 1]) continue;
+      const int cs = coop_smem(pp[q].spr, fp64 != 0, pp[q].ring_rows, pp[q].lpad, widths[k]);
+      if (((cs + 15) & ~15) <= kCoopSmemLimit) {
+        part[k].push_back(q);
+        taken++;
+        break;
+      }
+    }
+  }
+  // buckets in the order of their costliest point (each part is in cost order)
+  int ord[3] = {0, 1, 2};
+  auto rank = [&](int k) -> double { return part[k].empty() ? -1.0 : cost[part[k][0]]; };
+  std::stable_sort(ord, ord + 3, [&](int a, int b) { return rank(a) > rank(b); });
+  for (int k : ord) {
+    if (part[k].empty()) continue;
+    int sl = 1, nm = 1, nl = 0, cs = 0;
+    for (int32_t q : part[k]) {
+      sl = std::max(sl, slots[q]);
+      nm = std::max(nm, modes[q]);
+      nl = std::max(nl, nls[q]);
+      cs = std::max(cs, coop_smem(pp[q].spr, fp64 != 0, pp[q].ring_rows, pp[q].lpad,
+                                  widths[k]));
+    }
+    Bucket b;
+    b.shape = KernelShape{sl, nm, fp64, nl, 0};
+    b.shape.coop = widths[k];
+    b.smem = (cs + 15) & ~15;
+    int cb = 0;
+    if (occupancy_solve(b.shape, b.smem, &cb) != 0 || cb < 1) continue;  // one-warp path
+    b.offset = (int)members.size();
+    b.count = (int)part[k].size();
+    members.insert(members.end(), part[k].begin(), part[k].end());
+    heads.push_back(b);
+  }
+}
+
+// The library's rule for the multi-warp head: the points whose own serial bisection costs
+// more than the batch's share of one resident warp, i.e. the points that would still run
+// after the device has finished everything else.  The share takes a resident warp to do
+// 0.65 of the work of a warp alone on its SM (the 4096-speed sweep, bound by its total
+// work: 8 resident FP64 warps per SM did that of 5.8 lone warps, 13 FP32 ones that of 7.3).
+int coop_auto_head(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
+                   const std::vector<int>& slots, const std::vector<int>& modes,
+                   const std::vector<int>& nls, const std::vector<int>& grps, int fp64) {
+  const size_t n = cost.size();
+  if (n == 0) return 0;
+  std::vector<int32_t> byc(n);
+  std::iota(byc.begin(), byc.end(), 0);
+  std::stable_sort(byc.begin(), byc.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+  const int32_t m = byc[n / 2];  // a typical point's residency
+  KernelShape ks{slots[m], modes[m], fp64, nls[m], grps[m]};
+  int bps = 0;
+  if (occupancy_solve(ks, (smem[m] + 15) & ~15, &bps) != 0 || bps < 1) bps = 1;
+  double total = 0.0;
+  for (double c : cost) total += c;
+  const double share = total / ((double)ctx->sms * std::max(1.0, 0.65 * bps));
+  int head = 0;
+  while (head < (int)n && head < 2 * ctx->sms && cost[byc[head]] > share) head++;
+  return head;
+}
+
 // Orders the work items by cost (largest first) and groups them into buckets of similar
 // shared-memory need, each launched as its own persistent grid.
 //
-// Multi-warp bisection: the heaviest buckets of a plain solve, as long as their points
-// together number at most one per SM, run each point on `coop` warps of one block (the
-// latency tail of the slowest points; see solve_coop_kernel).  Buckets whose points pack
-// trials into lane groups keep them while their deepest trials fit in half a warp: that
-// speculation needs no extra warps.  pp (NULL for trial batches) gives the per-point sizes
-// the multi-warp shared memory follows from.
+// Multi-warp bisection (plain solves): the `coop_head` costliest points run each on
+// `coop_warps` warps of one block, as a bucket of their own ahead of the others (the
+// latency tail of the slowest points; see solve_coop_kernel and coop_head_bucket).  pp
+// (NULL for trial batches) gives the per-point sizes the multi-warp shared memory follows
+// from.
 int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<double>& cost,
                  const std::vector<int>& slots, const std::vector<int>& modes,
                  const std::vector<int>& nls, const std::vector<int>& grps, bool trials,
                  int fp64, int max_buckets,
                  std::vector<int32_t>& order, std::vector<Bucket>& buckets,
-                 const std::vector<PointParams>* pp = nullptr, int coop_warps = 1) {
-  const int nbmax = max_buckets > 0 ? std::min(max_buckets, kMaxBuckets) : kDefaultBuckets;
-  const size_t n = smem.size();
-  std::vector<int32_t> idx(n);
-  std::iota(idx.begin(), idx.end(), 0);
-  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return smem[a] > smem[b]; });
+                 const std::vector<PointParams>* pp = nullptr, int coop_warps = 1,
+                 int coop_head = 0) {
+  int nbmax = max_buckets > 0 ? std::min(max_buckets, kMaxBuckets) : kDefaultBuckets;
+  const size_t n_all = smem.size();
   buckets.clear();
   order.clear();
-  order.reserve(n);
-  if (n == 0) return MCS_OK;
-  const double hi = smem[idx.front()], lo = std::max(1, smem[idx.back()]);
+  order.reserve(n_all);
+  if (n_all == 0) return MCS_OK;
+  // resident blocks per SM and grid of a bucket, which then joins the list
+  auto place = [&](Bucket& b) -> int {
+    int bps = 0;
+    const int rc = trials ? occupancy_trials(b.shape, b.smem, &bps)
+                          : occupancy_solve(b.shape, b.smem, &bps);
+    if (rc != 0)
+      return fail(MCS_ERR_CUDA, "occupancy query failed: %s",
+                  cudaGetErrorString((cudaError_t)rc));
+    if (bps < 1)
+      return fail(MCS_ERR_UNSUPPORTED, "a %d-byte warp does not fit on an SM", b.smem);
+    b.blocks_per_sm = bps;
+    b.grid = (int)std::min<long long>(b.count, (long long)bps * ctx->sms);
+    buckets.push_back(b);
+    return MCS_OK;
+  };
+  int rc = MCS_OK;
+  std::vector<char> in_head(n_all, 0);
+  if (!trials && pp && coop_warps > 1 && coop_head > 0) {
+    std::vector<int32_t> members;
+    std::vector<Bucket> heads;
+    coop_head_buckets(cost, slots, modes, nls, grps, *pp, fp64, coop_warps, coop_head,
+                      members, heads);
+    order.insert(order.end(), members.begin(), members.end());
+    for (int32_t q : members) in_head[q] = 1;
+    for (Bucket& b : heads)
+      if ((rc = place(b))) return rc;
+    nbmax = std::min(nbmax, kMaxBuckets - (int)heads.size());
+  }
+  int classes = 0;
+  std::vector<int32_t> idx;
+  idx.reserve(n_all);
+  for (size_t q = 0; q < n_all; q++)
+    if (!in_head[q]) idx.push_back((int32_t)q);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return smem[a] > smem[b]; });
+  const size_t n = idx.size();
+  const double hi = n ? smem[idx.front()] : 1.0, lo = n ? std::max(1, smem[idx.back()]) : 1.0;
   // size classes: a bucket holds the points within a factor `ratio` of its largest need
   const double ratio = std::max(1.1, std::pow(hi / lo, 1.0 / nbmax) * 1.0001);
   size_t i = 0;
@@ -423,7 +543,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
       gr = std::max(gr, grps[idx[j]]);
       j++;
     }
-    if ((int)buckets.size() == nbmax - 1) {  // last bucket takes the rest
+    if (++classes == nbmax) {  // last bucket takes the rest
       for (size_t k = j; k < n; k++) {
         sl = std::max(sl, slots[idx[k]]);
         nm = std::max(nm, modes[idx[k]]);
@@ -439,44 +559,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
     b.smem = (top + 15) & ~15;
     b.shape = KernelShape{sl, nm, fp64, nl, trials ? 0 : gr};
     order.insert(order.end(), seg.begin(), seg.end());
-    // lane groups speculate without extra warps, but only while a trial's slices fit in a
-    // fraction of the warp: points whose deepest trials need more than half of it run
-    // their deep levels serially there, and take the multi-warp path like the others
-    int nz_top = 0;
-    if (pp)
-      for (int32_t q : seg) nz_top = std::max(nz_top, (*pp)[q].nz_max);
-    if (!trials && pp && coop_warps > 1 && (gr == 0 || nz_top > kWarp / 2) &&
-        (int)order.size() <= ctx->sms) {
-      // the widest block whose rings fit: the requested width, else 4, else 3
-      for (int wv : {coop_warps, 4, 3}) {
-        if (wv > coop_warps) continue;
-        int cs = 0;
-        for (int32_t q : seg) {
-          const PointParams& P = (*pp)[q];
-          cs = std::max(cs, coop_smem(P.spr, fp64 != 0, P.ring_rows, P.lpad, wv));
-        }
-        cs = (cs + 15) & ~15;
-        if (cs > kCoopSmemLimit) continue;
-        KernelShape ks = b.shape;
-        ks.coop = wv;
-        int cb = 0;
-        if (occupancy_solve(ks, cs, &cb) != 0 || cb < 1) continue;
-        b.shape = ks;
-        b.smem = cs;
-        break;
-      }
-    }
-    int bps = 0;
-    const int rc = trials ? occupancy_trials(b.shape, b.smem, &bps)
-                          : occupancy_solve(b.shape, b.smem, &bps);
-    if (rc != 0)
-      return fail(MCS_ERR_CUDA, "occupancy query failed: %s",
-                  cudaGetErrorString((cudaError_t)rc));
-    if (bps < 1)
-      return fail(MCS_ERR_UNSUPPORTED, "a %d-byte warp does not fit on an SM", b.smem);
-    b.blocks_per_sm = bps;
-    b.grid = (int)std::min<long long>(b.count, (long long)bps * ctx->sms);
-    buckets.push_back(b);
+    if ((rc = place(b))) return rc;
     i = j;
   }
   return MCS_OK;
@@ -663,18 +746,22 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   pl->ctx = ctx;
   pl->n = n_points;
   std::vector<int32_t> order;
-  // multi-warp bisection for plain solves.  By default (0) only for batches of at most
-  // kCoopAutoPerSm points per SM: there the slowest points' serial bisections are the whole
-  // call, while a larger batch is bound by its total work, to which the speculative trials
-  // add (the 4096-speed sweep measured 200 ms with it against 194 ms without).
-  constexpr int kCoopAutoPerSm = 4;
-  const bool coop_auto = n_points <= (size_t)kCoopAutoPerSm * ctx->sms;
-  const int coop = sur ? 1
-                   : o->coop_warps == 0 ? (coop_auto ? kCoopMaxWarpsHost : 1)
-                                        : o->coop_warps;
+  // multi-warp bisection for plain solves.  The library's rule (both options 0) gives it to
+  // the points whose serial bisections would outlast the rest of the batch (coop_auto_head);
+  // a batch bound by its total work gets none, since the speculative trials add to it.
+  int coop = 1, head = 0;
+  if (!sur) {
+    if (o->coop_warps == 0 && o->coop_points == 0) {
+      head = coop_auto_head(ctx, smem, cost, slots, modes, nls, grps, o->precision == MCS_FP64);
+      if (head > 0) coop = kCoopMaxWarpsHost;
+    } else if (o->coop_warps != 1) {
+      coop = o->coop_warps == 0 ? kCoopMaxWarpsHost : o->coop_warps;
+      head = o->coop_points == 0 ? ctx->sms : o->coop_points;
+    }
+  }
   rc = make_buckets(ctx, smem, cost, slots, modes, nls, grps, false, o->precision == MCS_FP64,
                     o->max_buckets, order,
-                    pl->buckets, &pp, coop);
+                    pl->buckets, &pp, coop, head);
   if (rc) {
     discard(pl);
     return rc;
@@ -769,6 +856,8 @@ void mcs_default_opts(mcs_opts* o) {
   o->max_buckets = 0;
   o->serial_trials = 0;
   o->coop_warps = 0;
+  o->coop_points = 0;
+  o->pad = 0;
 }
 
 const char* mcs_last_error(void) { return g_last_error.c_str(); }

@@ -83,7 +83,8 @@ class Opts(C.Structure):
                 ("revs", C.c_int32), ("nonlinear", C.c_int32), ("honor_runout", C.c_int32),
                 ("steps_per_tooth", C.c_int32), ("slices", C.c_int32),
                 ("chatter_idx", C.c_double), ("precision", C.c_int32),
-                ("max_buckets", C.c_int32), ("serial_trials", C.c_int32), ("coop_warps", C.c_int32)]
+                ("max_buckets", C.c_int32), ("serial_trials", C.c_int32), ("coop_warps", C.c_int32),
+                ("coop_points", C.c_int32), ("pad", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -232,9 +233,10 @@ def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
     plus the explicit extensions honorRunout, stepsPerTooth, slices, chatterIdx,
     precision ("fp64", the default: FP64 force law and modal integration; "fp32"), maxBuckets
     (the schedule; 0 = the library's default, see mcs.tune), coopWarps (warps sharing the
-    bisection of each of the heaviest points; 0 = the library's default, 1 = off) and
-    serialTrials (True: one
-    bisection trial at a time instead of speculative lane groups; same results)."""
+    bisection of each of the heaviest points; 0 = the library's default, 1 = off),
+    coopPoints (how many of the costliest points do so; 0 = one per SM) and serialTrials
+    (True: one bisection trial at a time instead of speculative lane groups; same
+    results)."""
     d = dict(DEFAULTS)
     if o:
         d.update(o)
@@ -245,7 +247,7 @@ def make_opts(o: Mapping[str, Any] | None = None, **kw) -> Opts:
                 int(d.get("stepsPerTooth", 0) or 0), int(d.get("slices", 0) or 0),
                 float(d.get("chatterIdx", CHATTER_IDX)), precision_code(d.get("precision")),
                 int(d.get("maxBuckets", 0) or 0), 1 if d.get("serialTrials", False) else 0,
-                int(d.get("coopWarps", 0) or 0))
+                int(d.get("coopWarps", 0) or 0), int(d.get("coopPoints", 0) or 0), 0)
 
 
 FP32 = 0
@@ -316,7 +318,8 @@ OPTS_DTYPE = np.dtype([("a_min", "<f8"), ("a_max", "<f8"), ("iters", "<i4"), ("r
                        ("nonlinear", "<i4"), ("honor_runout", "<i4"),
                        ("steps_per_tooth", "<i4"), ("slices", "<i4"), ("chatter_idx", "<f8"),
                        ("precision", "<i4"), ("max_buckets", "<i4"),
-                       ("serial_trials", "<i4"), ("coop_warps", "<i4")])
+                       ("serial_trials", "<i4"), ("coop_warps", "<i4"),
+                       ("coop_points", "<i4"), ("pad", "<i4")])
 for _d, _c in ((MODAL_DTYPE, Modal), (SETUP_DTYPE, Setup), (POINT_DTYPE, Point),
                (TRIAL_DTYPE, Trial), (OPTS_DTYPE, Opts)):
     assert _d.itemsize == C.sizeof(_c), (_d, _c)

@@ -204,7 +204,13 @@ static int parse_opts(napi_env env, napi_value v, mcs_opts* o) {
   o->revs = (int32_t)revs;
   o->steps_per_tooth = (int32_t)spt;
   o->slices = (int32_t)slices;
-  o->precision = strcmp(prec, "fp64") == 0 ? MCS_FP64 : MCS_FP32;
+  /* no precision given: the library's default (FP64, the reference's arithmetic) */
+  if (strcmp(prec, "fp32") == 0)
+    o->precision = MCS_FP32;
+  else if (strcmp(prec, "fp64") == 0)
+    o->precision = MCS_FP64;
+  else if (prec[0] != 0)
+    return -1;
   return 0;
 }
 

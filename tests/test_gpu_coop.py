@@ -35,8 +35,9 @@ def test_every_width_gives_the_serial_results(ctx, precision):
         assert got.tobytes() == ref.tobytes(), w
         plan = ctx.plan(wl.setups, wl.modals, wl.points, o)
         info = plan.info()
-        # the heaviest points, at most one per SM, take the multi-warp path
-        assert 0 < info["coop_points"] <= 148, info
+        # the heaviest points take the multi-warp path: one per SM for an explicit width,
+        # up to two per SM under the library's rule (a batch of 2.6 points per SM)
+        assert 0 < info["coop_points"] <= (2 * 148 if w == 0 else 148), info
         plan.execute()
         assert plan.results().tobytes() == ref.tobytes(), w
         plan.close()
@@ -44,6 +45,24 @@ def test_every_width_gives_the_serial_results(ctx, precision):
                                                           coop_warps=1))
     assert off.info()["coop_points"] == 0
     off.close()
+
+
+def test_library_rule_follows_the_tail(ctx):
+    """The library's rule gives the multi-warp path to the points that would outlast the
+    rest of their batch: none in the 4096-speed sweep (bound by its total work), the slow
+    low-speed points of a 768-speed sweep, and every point of an 18-point request."""
+    from mcs import workloads as W
+
+    def heads(wl):
+        plan = ctx.plan(wl.setups, wl.modals, wl.points, wl.opts)
+        n = plan.info()["coop_points"]
+        plan.close()
+        return n
+
+    assert heads(W.sweep()) == 0
+    n768 = heads(W.sweep(n_speeds=768))
+    assert 100 <= n768 <= 2 * 148, n768
+    assert heads(W.sweep(n_speeds=18)) == 18
 
 
 def test_small_batch_runs_every_point_on_several_warps(ctx):

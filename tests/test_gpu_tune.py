@@ -22,7 +22,9 @@ def test_results_identical_for_every_schedule(ctx):
         plan = ctx.plan(wl.setups, wl.modals, wl.points, o)
         plan.execute()
         assert plan.results().tobytes() == r.tobytes()
-        assert plan.info()["kernels"] <= nb
+        info = plan.info()
+        # the size classes, plus one multi-warp bucket per block width in use (at most 3)
+        assert info["kernels"] <= nb + (3 if info["coop_points"] else 0), info
         plan.close()
         if ref is None:
             ref = r

@@ -63,5 +63,7 @@ def test_old_option_records_read_with_defaults():
     old = np.frombuffer(bytes(o), dtype=np.uint8)[:56].copy()  # the 56-byte layout
     r = A.opts_from_record(old)
     assert r.max_buckets == 0 and r.serial_trials == 0 and r.a_max == o.a_max
-    assert C.sizeof(A.Opts) == 64
+    assert r.coop_warps == 0 and r.coop_points == 0
+    assert C.sizeof(A.Opts) == 72
     assert A.make_opts(serialTrials=True).serial_trials == 1
+    assert A.make_opts(coopWarps=3, coopPoints=40).coop_points == 40
