@@ -616,6 +616,8 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
     ga.info = static_cast<mcs_guide_info*>(pl->ginfo.p);
     ga.hw_min = pl->gopts.hw_min;
     ga.refine = pl->gopts.refine;
+    ga.mode = pl->gopts.mode;
+    ga.levels = pl->gopts.levels;
   }
   const bool forked = !captured && nb > 1;
   if (forked) MCS_CUDA(cudaEventRecord(ctx->fork, s0));
@@ -706,7 +708,9 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   int rc = check_inputs(setups, n_setups, modals, n_modals, points, n_points, o);
   if (rc) return rc;
   if (sur && (!g || !(g->z > 0) || !(g->hw_min > 0) || !(g->hw_max >= g->hw_min) ||
-              !(g->hw_direct > 0) || g->refine < 0 || g->refine > 30))
+              !(g->hw_direct > 0) || g->refine < 0 || g->refine > 30 ||
+              (g->mode != MCS_GUIDE_SPECULATE && g->mode != MCS_GUIDE_BRACKET) ||
+              (g->mode == MCS_GUIDE_SPECULATE && g->levels < 1)))
     return fail(MCS_ERR_ARG, "guide options out of range");
   std::vector<PointParams> pp(n_points);
   std::vector<int> smem(n_points), slots(n_points), modes(n_points), nls(n_points),

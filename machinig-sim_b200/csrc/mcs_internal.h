@@ -112,6 +112,8 @@ struct GuideArgs {
   mcs_guide_info* info = nullptr; // per point path taken
   float hw_min = 0.f;             // half-width the refinement count is calibrated on
   int refine = 0;                 // halvings of a hw_min bracket
+  int mode = 0;                   // MCS_GUIDE_SPECULATE or MCS_GUIDE_BRACKET
+  int levels = 0;                 // speculate: bisection levels
 };
 
 // One chatterAt trial of the batch kernel.

@@ -607,6 +607,122 @@ __device__ __forceinline__ void tree_midpoints(double lo, double hi, int d, doub
   }
 }
 
+// The lanes a trial at depth ap takes in a lane group (pack_groups' rule).
+__device__ __forceinline__ int group_lanes(const PointParams* __restrict__ P, double ap) {
+  int nz;
+  double dz;
+  slice_rule(P, ap, nz, dz);
+  int sz = 2;
+  while (sz < nz) sz <<= 1;
+  return sz;
+}
+
+// First fit of an aligned block of sz lanes into the used mask, and the number of empty
+// groups that then cover the free lanes: the packing of pack_groups, one trial at a time.
+__device__ __forceinline__ bool fit_block(unsigned& used, int sz, int trials) {
+  if (sz > kWarp) return false;
+  const unsigned mask = sz == kWarp ? 0xffffffffu : ((1u << sz) - 1u);
+  int off = -1;
+  for (int o = 0; o < kWarp; o += sz)
+    if ((used & (mask << o)) == 0u) {
+      off = o;
+      break;
+    }
+  if (off < 0) return false;
+  unsigned u = used | (mask << off);
+  int ng = trials;
+  for (int s = 16; s >= 2; s >>= 1)
+    for (int o = 0; o < kWarp; o += s) {
+      const unsigned m = (1u << s) - 1u;
+      if ((u & (m << o)) == 0u) {
+        u |= m << o;
+        ng++;
+      }
+    }
+  if (ng > kMaxGroups) return false;
+  used |= mask << off;
+  return true;
+}
+
+// Where the next bisection levels are expected to go: with a surrogate, a normal
+// distribution of the log critical depth (mean mu, standard deviation sigma); without one
+// every log depth of [a_min, a_max] alike, so that a node counts by its bracket's width.
+struct Prior {
+  bool normal;
+  double mu, inv_sigma;
+};
+
+// Probability weight of the node bracketing [l, h]: the brackets touching a_min or a_max
+// take the mass beyond them too.
+__device__ __forceinline__ double node_weight(const Prior& pr, double l, double h,
+                                              double a_min, double a_max) {
+  if (!pr.normal) return log(h / l);
+  const double a = l <= a_min ? -INFINITY : (log(l) - pr.mu) * pr.inv_sigma;
+  const double b = h >= a_max ? INFINITY : (log(h) - pr.mu) * pr.inv_sigma;
+  return normcdf(b) - normcdf(a);
+}
+
+// The trials of one speculative round: nodes of the remaining bisection tree of [lo, hi],
+// node 0 the next midpoint, chosen best first by their weight under the prior while their
+// lane groups fit in the warp.  A node's children are candidates once it is chosen, and a
+// child never outweighs its parent, so the chosen nodes form a subtree containing node 0;
+// kid[k][0] is the node taken when node k chatters (the bracket [l, m]), kid[k][1] the one
+// taken when it is stable, -1 where the round's walk stops.  The midpoints are the square
+// roots the serial bisection takes, so the walk decides exactly what one trial at a time
+// would.  n = 0: even node 0 needs more than the warp's lanes.
+struct SpecPlan {
+  int n;
+  double m[kMaxGroups];
+  signed char kid[kMaxGroups][2];
+};
+
+__device__ __noinline__ void plan_round(const PointParams* __restrict__ P, double lo, double hi,
+                                        int levels, const Prior& pr, double a_min,
+                                        double a_max, SpecPlan& sp) {
+  constexpr int kCand = 2 * kMaxGroups + 1;
+  double cl[kCand], ch[kCand], cw[kCand];
+  signed char cpar[kCand], cside[kCand], cdep[kCand];
+  bool alive[kCand];
+  int nc = 1;
+  cl[0] = lo;
+  ch[0] = hi;
+  cw[0] = 1.0;
+  cpar[0] = -1;
+  cside[0] = 0;
+  cdep[0] = 0;
+  alive[0] = true;
+  sp.n = 0;
+  unsigned used = 0u;
+  for (;;) {
+    int best = -1;
+    for (int c = 0; c < nc; c++)
+      if (alive[c] && (best < 0 || cw[c] > cw[best])) best = c;
+    if (best < 0 || sp.n >= kMaxGroups) break;
+    alive[best] = false;
+    const double l = cl[best], h = ch[best], m = sqrt(l * h);
+    if (!fit_block(used, group_lanes(P, m), sp.n + 1)) {
+      if (sp.n == 0) break;  // node 0 does not fit: one trial on the whole warp
+      continue;
+    }
+    const int k = sp.n++;
+    sp.m[k] = m;
+    sp.kid[k][0] = sp.kid[k][1] = -1;
+    if (cpar[best] >= 0) sp.kid[cpar[best]][cside[best]] = (signed char)k;
+    if (cdep[best] + 1 < levels && nc + 2 <= kCand) {
+      for (int s = 0; s < 2; s++) {
+        cl[nc] = s == 0 ? l : m;
+        ch[nc] = s == 0 ? m : h;
+        cw[nc] = node_weight(pr, cl[nc], ch[nc], a_min, a_max);
+        cpar[nc] = (signed char)k;
+        cside[nc] = (signed char)s;
+        cdep[nc] = (signed char)(cdep[best] + 1);
+        alive[nc] = true;
+        nc++;
+      }
+    }
+  }
+}
+
 // One trial on the whole warp.
 template <typename T, int SLOTS, int NM, bool NL>
 __device__ __forceinline__ TrialOut simulate_trial(const PointParams* __restrict__ P,
@@ -686,19 +802,28 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
       // timeDomainLimit (stabtd.js:24-32) as a state machine of rounds around ONE call of
       // the trial code (inlined once).  A round is one trial on the whole warp, or several
       // trials of this point in lane groups: the next bisection levels run speculatively
-      // (the midpoints of a subtree, computed by the same square roots the serial
-      // bisection takes), and only the trials on the decision path are counted, so the
-      // results are those of one trial at a time.  The states: the plain first trial at
-      // a_max, then either the plain geometric bisection over [a_min, a_max] or, with a
-      // surrogate guide, the bracket exp(mu -+ hw) kept inside [a_min, a_max], verified at
-      // its upper (chatter) and lower (stable) end and refined by the same bisection.  A
-      // failed verification falls back to the plain bisection, whose a_max trial has
-      // already run.
+      // (nodes of the remaining bisection tree, chosen by plan_round, whose midpoints are
+      // the same square roots the serial bisection takes), and only the trials on the
+      // decision path are counted, so the results are those of one trial at a time.  The
+      // states: the plain first trial at a_max, then either the plain geometric bisection
+      // over [a_min, a_max] (with a speculating guide: for g.levels levels, its rounds
+      // spent where the prediction puts the limit) or, with a bracket guide, the bracket
+      // exp(mu -+ hw) kept inside [a_min, a_max], verified at its upper (chatter) and
+      // lower (stable) end and refined by the same bisection.  A failed verification
+      // falls back to the plain bisection, whose a_max trial has already run.
       enum : int { kTop, kGuideHi, kGuideLo, kBisect, kDone };
-      const bool guided = g.guide != nullptr && g.guide[pi].y >= 0.f;
+      const bool speculate = g.guide != nullptr && g.mode == MCS_GUIDE_SPECULATE;
+      const bool guided = g.guide != nullptr && (speculate || g.guide[pi].y >= 0.f);
       const bool can_group = GR && P->groups > 1;
       int path = guided ? MCS_PATH_GUIDED : MCS_PATH_DIRECT;
-      int state = kTop, it = 0, iters = o.iters;
+      // where the speculative rounds look: the bracket widths, or the prediction
+      Prior prior;
+      prior.normal = false;
+      prior.mu = 0.0;
+      prior.inv_sigma = 0.0;
+      SpecPlan sp;
+      sp.n = 0;
+      int state = kTop, it = 0, iters = o.iters, nrounds = 0;
       double lo = o.a_min, hi = o.a_max, glo = 0.0, ghi = 0.0;
       // enter the bisection of [l, h] for n iterations
       auto bisect = [&](double l, double h, int nit) {
@@ -724,7 +849,6 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         // ---- plan the round ----
         Groups G;
         one_group(G, 0.0);
-        int levels = 0;       // bisection levels the round decides
         bool packed = false;  // guide check: the lower end (and spec refinement levels) too
         int spec = 0;
         if (state == kBisect) {
@@ -742,18 +866,14 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
             r.hi = hi;
             break;
           }
-          const int lv = min(4, iters - it);
-          levels = 1;
-          if (can_group && lv >= 2) {
-            double m[15];  // the speculative subtree, 4 levels at most
-            tree_midpoints(lo, hi, lv, m);
-            for (int d = lv; d >= 2; d--)
-              if (pack_groups(P, m, (1 << d) - 1, G)) {
-                levels = d;
-                break;
-              }
+          // the next midpoint and, in lane groups beside it, the further nodes of the
+          // remaining tree the prior weighs most (the same first-fit packing accepts them)
+          sp.n = 0;
+          if (can_group && iters - it >= 2) {
+            plan_round(P, lo, hi, iters - it, prior, o.a_min, o.a_max, sp);
+            if (sp.n < 2 || !pack_groups(P, sp.m, sp.n, G)) sp.n = 0;
           }
-          if (levels == 1) G.ap[0] = sqrt(lo * hi);
+          if (sp.n == 0) G.ap[0] = sqrt(lo * hi);
         } else if (state == kTop) {
           G.ap[0] = o.a_max;
         } else if (state == kGuideHi) {
@@ -779,11 +899,13 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         }
         // ---- run ----
         simulate<T, SLOTS, NM, NL, GR>(P, G, table, ring, samples, outs, lane);
+        nrounds++;
         // ---- decide ----
         if (state == kBisect) {
-          // walk the decision path: node k's midpoint is the serial bisection's sqrt(lo*hi)
+          // walk the decision path through the round's nodes: node k's midpoint is the
+          // serial bisection's sqrt(lo*hi) at that point of the path
           int node = 0;
-          for (int d = 0; d < levels; d++) {
+          do {
             const double mid = sqrt(lo * hi);
             const bool c = account(outs[node]);
             if (c)
@@ -791,8 +913,8 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
             else
               lo = mid;
             it++;
-            node = 2 * node + (c ? 1 : 2);
-          }
+            node = sp.n == 0 ? -1 : sp.kid[node][c ? 0 : 1];
+          } while (node >= 0 && it < iters);
         } else if (state == kTop) {
           const bool c = account(outs[0]);
           if (!c) {
@@ -804,6 +926,13 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
             state = kDone;
           } else if (!guided) {
             bisect(o.a_min, o.a_max, o.iters);
+          } else if (speculate) {
+            // the plain bisection for `levels` levels, its rounds steered by N(mu, sigma)
+            const double sg = g.sigma != nullptr ? (double)g.sigma[pi] : 1.0;
+            prior.normal = true;
+            prior.mu = (double)g.guide[pi].x;
+            prior.inv_sigma = 1.0 / fmax(sg, 1e-3);
+            bisect(o.a_min, o.a_max, min(g.levels, o.iters));
           } else {
             const float2 gd = g.guide[pi];
             const double hw = (double)gd.y;
@@ -862,7 +991,7 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         gi.mu = g.guide ? g.guide[pi].x : 0.f;
         gi.sigma = g.sigma ? g.sigma[pi] : 0.f;
         gi.path = path;
-        gi.pad = 0;
+        gi.rounds = nrounds;
         g.info[pi] = gi;
       }
     }

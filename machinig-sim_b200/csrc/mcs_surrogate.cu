@@ -739,6 +739,8 @@ void mcs_default_guide_opts(mcs_guide_opts* o) {
   o->hw_max = 0.40546511f;  // log(1.5)
   o->hw_direct = 0.69314718f;  // log(2)
   o->refine = 3;
+  o->mode = MCS_GUIDE_SPECULATE;
+  o->levels = 8;
   o->pad = 0;
 }
 

@@ -366,13 +366,19 @@ class TrainOpts(C.Structure):
 
 class GuideOpts(C.Structure):
     _fields_ = [("z", C.c_float), ("hw_min", C.c_float), ("hw_max", C.c_float),
-                ("hw_direct", C.c_float), ("refine", C.c_int32), ("pad", C.c_int32)]
+                ("hw_direct", C.c_float), ("refine", C.c_int32), ("mode", C.c_int32),
+                ("levels", C.c_int32), ("pad", C.c_int32)]
+
+
+GUIDE_SPECULATE = 0
+GUIDE_BRACKET = 1
 
 
 class GuideInfo(C.Structure):
     _fields_ = [("mu", C.c_float), ("sigma", C.c_float), ("path", C.c_int32),
-                ("pad", C.c_int32)]
+                ("rounds", C.c_int32)]
 
 
-GUIDE_INFO_DTYPE = np.dtype([("mu", "<f4"), ("sigma", "<f4"), ("path", "<i4"), ("pad", "<i4")])
+GUIDE_INFO_DTYPE = np.dtype([("mu", "<f4"), ("sigma", "<f4"), ("path", "<i4"),
+                             ("rounds", "<i4")])
 assert GUIDE_INFO_DTYPE.itemsize == C.sizeof(GuideInfo)

@@ -142,11 +142,13 @@ def trained_small(ctx):
 
 
 def wide_guide():
-    """Default guide options, but no point goes straight to the plain bisection, so
-    that every path is exercised whatever the small model's sigma."""
+    """The bracket method with its default options, but no point goes straight to the
+    plain bisection, so that every path is exercised whatever the small model's sigma."""
+    from mcs import _abi as A
     from mcs._lib import default_guide_opts
 
     g = default_guide_opts()
+    g.mode = A.GUIDE_BRACKET
     g.hw_direct = 100.0
     g.hw_max = math.log(2.0)
     return g
@@ -201,13 +203,73 @@ def test_guided_solve_against_plain(ctx, trained_small):
     assert np.all(np.isfinite(info["mu"])) and np.all(info["sigma"] > 0)
 
 
-def test_direct_guide_reproduces_plain(ctx, trained_small):
-    """A tiny hw_direct sends every point to the plain bisection: the plain results."""
+def plain_bracket_after(lo_final, hi_final, a_min, a_max, levels):
+    """The plain geometric bisection's bracket after `levels` levels on the way to its
+    final bracket (every decision of the path is the side the final bracket lies on)."""
+    lo = np.full(len(lo_final), a_min)
+    hi = np.full(len(lo_final), a_max)
+    for _ in range(levels):
+        m = np.sqrt(lo * hi)
+        c = hi_final <= m
+        hi = np.where(c, m, hi)
+        lo = np.where(c, lo, m)
+    return lo, hi
+
+
+def test_speculative_guide_is_the_plain_bisection(ctx, trained_small):
+    """The default guided method runs the plain bisection's own trials, steered by the
+    prediction: after `levels` levels its bracket is exactly the plain bisection's, so the
+    limit lies within half that bracket's width of the plain limit (1.12 % for 8 of the
+    10 levels over [0.05, 15]); with levels = iters the results are the plain ones byte for
+    byte."""
     from mcs import _abi as A
     from mcs._lib import default_guide_opts
 
     s, wl, plain = trained_small
     g = default_guide_opts()
+    assert g.mode == A.GUIDE_SPECULATE and g.levels == 8
+    res, info = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts, g)
+    op = plain["open"] == 1
+    assert np.array_equal(res["open"], plain["open"])
+    for f in ("alim", "lo", "hi", "trials"):
+        assert np.array_equal(res[f][op], plain[f][op]), f
+    assert np.all(info["path"][op] == A.PATH_OPEN)
+    assert np.all(info["path"][~op] == A.PATH_GUIDED)
+    lo8, hi8 = plain_bracket_after(plain["lo"][~op], plain["hi"][~op], wl.opts.a_min,
+                                   wl.opts.a_max, 8)
+    assert np.array_equal(res["lo"][~op], lo8) and np.array_equal(res["hi"][~op], hi8)
+    assert np.array_equal(res["alim"][~op], np.sqrt(lo8 * hi8))
+    half = math.exp(math.log(wl.opts.a_max / wl.opts.a_min) / 2 ** 9) - 1
+    assert np.all(np.abs(res["alim"][~op] / plain["alim"][~op] - 1) <= half * (1 + 1e-9))
+    assert np.all(res["trials"][~op] == 1 + 8)
+    assert np.all((info["rounds"] >= 1) & (info["rounds"] <= res["trials"]))
+    print(f"speculative: rounds {info['rounds'].sum()} for {res['trials'].sum()} trials")
+    # all the levels: the plain solve, byte for byte
+    g.levels = wl.opts.iters
+    full, finfo = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts, g)
+    assert full.tobytes() == plain.tobytes()
+    # a levels value above iters means iters
+    g.levels = 99
+    again, _ = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts, g)
+    assert again.tobytes() == plain.tobytes()
+    # serial trials: one trial per round, the same results
+    o = wl.opts.__class__.from_buffer_copy(wl.opts)
+    o.serial_trials = 1
+    g.levels = 8
+    ser, sinfo = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, o, g)
+    assert ser.tobytes() == res.tobytes()
+    assert np.array_equal(sinfo["rounds"], ser["trials"])
+
+
+def test_direct_guide_reproduces_plain(ctx, trained_small):
+    """With the bracket method, a tiny hw_direct sends every point to the plain bisection:
+    the plain results."""
+    from mcs import _abi as A
+    from mcs._lib import default_guide_opts
+
+    s, wl, plain = trained_small
+    g = default_guide_opts()
+    g.mode = A.GUIDE_BRACKET
     g.hw_direct = 1e-6
     res, info = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts, g)
     assert np.all(info["path"] == A.PATH_DIRECT)
@@ -275,14 +337,44 @@ def test_keep_best_and_warm_start(ctx, feats):
     s.close()
 
 
-def test_ablation_trained_model_saves_trials(ctx):
+def test_ablation_trained_model_saves_rounds(ctx):
     """What the trained network gains over the method without it.  On 2048 serving
-    queries the committed model's guided solve needs fewer time-domain trials than the
-    plain bisection, and than the same guided method with an untrained network, while its
-    limits stay within 2 % of the plain ones on at least 99 % of the queries."""
+    queries the speculative guided solve with the committed model needs fewer rounds (warp
+    passes over the trial loop, the point's cost in time) than the same solve steered by an
+    untrained network, with the same limits: both are the plain bisection's after 8
+    levels, within 1.12 % of the plain limits."""
     from mcs import Surrogate
     from mcs import surrogate as SG
     from mcs import workloads as W
+
+    assert SG.DEFAULT_MODEL.exists(), "the trained model is part of the package"
+    sv = W.serve().subset(np.arange(2048))
+    plain = ctx.solve(sv.setups, sv.modals, sv.points, sv.opts)
+    trained = SG.load(ctx)
+    untrained = Surrogate(ctx, 1)
+    rt, it = ctx.solve_guided(trained, sv.setups, sv.modals, sv.points, sv.opts)
+    ru, iu = ctx.solve_guided(untrained, sv.setups, sv.modals, sv.points, sv.opts)
+    assert rt.tobytes() == ru.tobytes()
+    rel = np.abs(rt["alim"] / plain["alim"] - 1)
+    nt, nu = int(it["rounds"].sum()), int(iu["rounds"].sum())
+    print(f"rounds: trained {nt}, untrained {nu} ({nt / nu:.3f}); max |alim / plain - 1| "
+          f"{rel.max():.4f}")
+    assert nt < 0.95 * nu
+    assert rel.max() <= 0.0113
+    trained.close()
+    untrained.close()
+
+
+def test_ablation_trained_model_saves_trials(ctx):
+    """The bracket method: on 2048 serving queries the committed model's guided solve
+    needs fewer time-domain trials than the plain bisection, and than the same guided
+    method with an untrained network, while its limits stay within 2 % of the plain ones
+    on at least 99 % of the queries."""
+    from mcs import Surrogate
+    from mcs import _abi as A
+    from mcs import surrogate as SG
+    from mcs import workloads as W
+    from mcs._lib import default_guide_opts
 
     assert SG.DEFAULT_MODEL.exists(), "the trained model is part of the package"
     sv = W.serve().subset(np.arange(2048))
@@ -294,8 +386,10 @@ def test_ablation_trained_model_saves_trials(ctx):
         op = (r["open"] == 1) & (plain["open"] == 1)
         return float(np.mean(op | (np.abs(r["alim"] / plain["alim"] - 1) <= 0.02)))
 
-    rt, it = ctx.solve_guided(trained, sv.setups, sv.modals, sv.points, sv.opts)
-    ru, iu = ctx.solve_guided(untrained, sv.setups, sv.modals, sv.points, sv.opts)
+    g = default_guide_opts()
+    g.mode = A.GUIDE_BRACKET
+    rt, it = ctx.solve_guided(trained, sv.setups, sv.modals, sv.points, sv.opts, g)
+    ru, iu = ctx.solve_guided(untrained, sv.setups, sv.modals, sv.points, sv.opts, g)
     tp, tt, tu = plain["trials"].sum(), rt["trials"].sum(), ru["trials"].sum()
     print(f"trials: plain {tp}, trained {tt} ({tt / tp:.3f}), untrained {tu} ({tu / tp:.3f}); "
           f"guided fraction trained {np.mean(it['path'] == 0):.3f} untrained "

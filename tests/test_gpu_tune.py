@@ -74,6 +74,7 @@ def test_lane_group_trials_match_serial_trials(ctx):
     from mcs import _abi as A
     from mcs import surrogate as SG
     from mcs import workloads as W
+    from mcs._lib import default_guide_opts
 
     wl = W.hetero(n=1024, first_seed=31337)
     serial = A.Opts.from_buffer_copy(bytes(wl.opts))
@@ -86,9 +87,18 @@ def test_lane_group_trials_match_serial_trials(ctx):
     assert plan.results().tobytes() == a.tobytes()
     plan.close()
     s = SG.load(ctx)
-    ga, ia = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, serial)
-    gb, ib = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts)
-    assert ga.tobytes() == gb.tobytes() and ia.tobytes() == ib.tobytes()
+    for mode in (A.GUIDE_SPECULATE, A.GUIDE_BRACKET):
+        g = default_guide_opts()
+        g.mode = mode
+        ga, ia = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, serial, g)
+        gb, ib = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts, g)
+        assert ga.tobytes() == gb.tobytes()
+        for f in ("mu", "sigma", "path"):
+            assert np.array_equal(ia[f], ib[f]), f
+        # one trial per round serially; lane groups take fewer rounds, never more
+        assert np.array_equal(ia["rounds"], ga["trials"])
+        assert np.all(ib["rounds"] <= ia["rounds"])
+        assert ib["rounds"].sum() < ia["rounds"].sum()
     s.close()
     with pytest.raises(Exception):
         bad = A.Opts.from_buffer_copy(bytes(wl.opts))
