@@ -645,7 +645,27 @@ def ours(args) -> int:
                              f"{len(idx)}-point subset",
                 **{f"within_2pct_of_cpu_fp64_{p}": within(v["res"][idx], r64)
                    for p, v in var.items()}}
+            if wl.opts.honor_runout:
+                rec["accuracy"]["runout_zero"] = runout_zero(wl, idx, r64, head["opts"])
         return rec
+
+    def runout_zero(wl, idx, r64, opts) -> dict:
+        """The reference's own chatterAt forces the runout to 0 (stabtd.js:16): the same
+        subset solved that way on the GPU and by the FP64 restatement, and how far the
+        runout the workload honours moves the limits."""
+        import dataclasses
+
+        o0 = A.Opts.from_buffer_copy(bytes(opts))
+        o0.honor_runout = 0
+        o0.precision = A.FP64
+        g0 = ctx.solve(wl.setups, wl.modals, wl.points[idx], o0)
+        h0, dt = run_oracle(dataclasses.replace(wl, opts=o0), idx, cpu_cores())
+        both = (h0["open"] == 1) & (r64["open"] == 1)
+        moved = np.where(both, 0.0, np.abs(h0["alim"] / r64["alim"] - 1))
+        return {"points": len(idx), "within_2pct_of_cpu_fp64_fp64": within(g0, h0),
+                "median_rel_change_by_runout": float(np.median(moved)),
+                "changed_over_2pct_by_runout": float(np.mean(moved > 0.02)),
+                "host_seconds": round(dt, 1)}
 
     def summarize(name: str, rec: dict, precision: str) -> dict:
         v = rec["var"][precision]

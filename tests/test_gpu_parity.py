@@ -32,7 +32,7 @@ pytestmark = pytest.mark.gpu
 
 DECISION_BAND = 0.02
 DEPTH_RTOL = 0.02
-DEPTH_QUANTILE = {"fp64": 0.98, "fp32": 0.95}
+DEPTH_QUANTILE = {"fp64": 0.99, "fp32": 0.95}
 MIN_AGREE = {"fp64": 0.99, "fp32": 0.97}
 INDEX_RTOL = 2e-3
 INDEX_ATOL = 1e-4
