@@ -1,9 +1,9 @@
 // The learned surrogate: an MLP 20 -> 256 -> 256 -> 256 -> 2 (SiLU) trained with a
 // Gaussian negative log-likelihood on log critical depths the time-domain solver
 // produced.  Weights and activations are BF16 and every product accumulates in FP32; the
-// Adam state and master weights are FP32.  Training (forward, backward, Adam) runs on
-// mma.sync m16n8k16 GEMMs with strided operands; inference runs in one fused kernel on
-// the 5th-generation tensor cores (tcgen05.mma with the accumulator in tensor memory).
+// Adam state and master weights are FP32.  Both run on the 5th-generation tensor cores
+// (tcgen05.mma with the accumulator in tensor memory): training (forward, backward, Adam)
+// through one GEMM kernel with strided operands, inference in one fused kernel.
 //
 // Layers are padded to tensor-core shapes: the 20 inputs to 32, the 2 outputs to 16;
 // padded weights start at zero and get zero gradients, so they stay zero.
@@ -51,82 +51,6 @@ struct Layout {
 const Layout kLay;
 
 // ---------------------------------------------------------------- kernels
-__device__ __forceinline__ uint16_t bf_bits(const bf16* p, long i, bool ok) {
-  return ok ? __bfloat16_as_ushort(p[i]) : (uint16_t)0;
-}
-__device__ __forceinline__ uint32_t pack2(uint16_t lo, uint16_t hi) {
-  return (uint32_t)lo | ((uint32_t)hi << 16);
-}
-
-// C[M x N] (+)= A[M x K] * B[K x N]; A(m, k) = A[m*sAm + k*sAk], B(k, n) = B[k*sBk + n*sBn]
-// (strides express the transposes of the backward pass).  4 warps per block, each a
-// 32 x 32 tile as 2 x 4 mma.sync.m16n8k16 (BF16 in, FP32 accumulate).
-__global__ void __launch_bounds__(128) gemm_bf16(const bf16* __restrict__ A, long sAm, long sAk,
-                                                 const bf16* __restrict__ B, long sBk, long sBn,
-                                                 float* __restrict__ C, long ldc, int M, int N,
-                                                 int K, int accumulate) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const int m0 = blockIdx.y * 64 + (warp & 1) * 32;
-  const int n0 = blockIdx.x * 64 + (warp >> 1) * 32;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += 16) {
-    uint32_t a[2][4], b[4][2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-      const int r0 = m0 + 16 * i + g, r1 = r0 + 8;
-      const int c0 = k0 + 2 * t, c1 = c0 + 8;
-      const bool v00 = r0 < M && c0 < K, v01 = r0 < M && c0 + 1 < K;
-      const bool v10 = r1 < M && c0 < K, v11 = r1 < M && c0 + 1 < K;
-      const bool w00 = r0 < M && c1 < K, w01 = r0 < M && c1 + 1 < K;
-      const bool w10 = r1 < M && c1 < K, w11 = r1 < M && c1 + 1 < K;
-      a[i][0] = pack2(bf_bits(A, r0 * sAm + c0 * sAk, v00), bf_bits(A, r0 * sAm + (c0 + 1) * sAk, v01));
-      a[i][1] = pack2(bf_bits(A, r1 * sAm + c0 * sAk, v10), bf_bits(A, r1 * sAm + (c0 + 1) * sAk, v11));
-      a[i][2] = pack2(bf_bits(A, r0 * sAm + c1 * sAk, w00), bf_bits(A, r0 * sAm + (c1 + 1) * sAk, w01));
-      a[i][3] = pack2(bf_bits(A, r1 * sAm + c1 * sAk, w10), bf_bits(A, r1 * sAm + (c1 + 1) * sAk, w11));
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int n = n0 + 8 * j + g;
-      const int k = k0 + 2 * t;
-      const bool vn = n < N;
-      b[j][0] = pack2(bf_bits(B, k * sBk + n * sBn, vn && k < K),
-                      bf_bits(B, (k + 1) * sBk + n * sBn, vn && k + 1 < K));
-      b[j][1] = pack2(bf_bits(B, (k + 8) * sBk + n * sBn, vn && k + 8 < K),
-                      bf_bits(B, (k + 9) * sBk + n * sBn, vn && k + 9 < K));
-    }
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        asm volatile(
-            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
-            "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-            : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]),
-              "r"(b[j][1]));
-  }
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int r = m0 + 16 * i + g + (e >= 2 ? 8 : 0);
-        const int c = n0 + 8 * j + 2 * t + (e & 1);
-        if (r < M && c < N) {
-          float* o = C + (long)r * ldc + c;
-          *o = accumulate ? *o + acc[i][j][e] : acc[i][j][e];
-        }
-      }
-}
-
 __device__ __forceinline__ float sigmoid(float z) { return 1.f / (1.f + __expf(-z)); }
 
 // z = C + bias (kept for the backward pass); out = BF16(silu(z)) or, for the last layer,
@@ -476,6 +400,241 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                  : "memory");
 }
 
+// ------------------------------------------------ training GEMMs on the tensor cores
+// C[M x N] (+)= A[M x K] B[K x N] with A(m, k) = A[m*sAm + k*sAk] and B(k, n) = B[k*sBk +
+// n*sBn] (the strides express the transposes of the backward pass), BF16 operands and an
+// FP32 accumulator in tensor memory.  One CTA of 4 warps owns a 128-row x nt-column tile of
+// C (nt = 16 ... 256, a multiple of 16) and runs over K in chunks of 64: the threads copy
+// the chunk's A rows and B columns into a shared-memory stage in the K-major operand layout
+// of mlp_infer_tc (rows past M, columns past N and k past K are zero), one thread issues
+// the chunk's tcgen05.mma (K = 16 each) and commits them to the stage's mbarrier.  Two
+// stages: the copy of the next chunk overlaps the MMAs of the current one, and a stage is
+// refilled only after its mbarrier says the MMAs that read it are done.  The four warps
+// read their 32 accumulator rows back with tcgen05.ld.  Every wait is bounded; a timeout
+// sets *err and the kernel drains its MMAs (bounded) before it frees the tensor memory.
+constexpr int kGtKc = 64;                                  // K per stage
+constexpr int kGtStageA = kTcRows * kGtKc * 2;             // 16 KB
+constexpr int kGtStageB = kTcCols * kGtKc * 2;             // 32 KB at nt = 256
+constexpr int kGtSmem = 2 * (kGtStageA + kGtStageB) + 64;  // stages + 2 mbarriers + TMEM slot
+
+// One operand chunk: rows [r0, r0 + R) of an operand X(r, k) = X[r*sr + k*sk] with r < rmax
+// and k in [k0, k0 + kc) with k < kmax (zero elsewhere), into dst in the K-major operand
+// layout (element (r, k) at ((k / 8) * R + r) * 8 + k % 8: the 8 k of a row and group are
+// 16 contiguous bytes).  The work item of a thread is an 8-k group:
+//   * k contiguous in X (sk == 1): one 16-byte load and one 16-byte store per (row, group);
+//   * rows contiguous (sr == 1): an 8-row x 8-k block, eight 16-byte loads along the rows,
+//     transposed in registers into eight 16-byte stores;
+//   * otherwise, or where a vector would leave the bounds or its 16-byte alignment,
+//     element by element.
+__device__ __forceinline__ uint16_t bf_at(const bf16* p, long i) {
+  return __bfloat16_as_ushort(p[i]);
+}
+
+__device__ __forceinline__ void stage_operand(const bf16* __restrict__ X, long sr, long sk,
+                                              int r0, int rmax, int k0, int kmax, int R,
+                                              int kc, uint16_t* __restrict__ dst, int tid) {
+  const int groups = kc / 8;
+  const bool base16 = (reinterpret_cast<uintptr_t>(X) & 15u) == 0;
+  if (sk == 1) {
+    // all of a thread's loads (at most 16: 256 rows x 8 groups over 128 threads) are issued
+    // before its stores
+    constexpr int kItems = kTcCols * (kGtKc / 8) / kTcThreads;
+    const bool vec = base16 && (sr % 8) == 0;
+    const int items = R * groups;
+    uint4 q[kItems];
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
+      const int e = tid + it * kTcThreads;
+      q[it] = make_uint4(0u, 0u, 0u, 0u);
+      const int r = e / groups, g = e - r * groups;
+      const int gr = r0 + r, gk = k0 + 8 * g;
+      if (e < items && gr < rmax) {
+        if (vec && gk + 8 <= kmax) {
+          q[it] = *reinterpret_cast<const uint4*>(X + gr * sr + gk);
+        } else {
+          uint16_t v[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) v[j] = gk + j < kmax ? bf_at(X, gr * sr + gk + j) : 0;
+          q[it].x = v[0] | ((uint32_t)v[1] << 16);
+          q[it].y = v[2] | ((uint32_t)v[3] << 16);
+          q[it].z = v[4] | ((uint32_t)v[5] << 16);
+          q[it].w = v[6] | ((uint32_t)v[7] << 16);
+        }
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
+      const int e = tid + it * kTcThreads;
+      const int r = e / groups, g = e - r * groups;
+      if (e < items) *reinterpret_cast<uint4*>(dst + ((size_t)g * R + r) * 8) = q[it];
+    }
+  } else {
+    const bool vec = base16 && sr == 1 && (sk % 8) == 0;
+    const int rb = R / 8;  // 8-row blocks
+    for (int e = tid; e < rb * groups; e += kTcThreads) {
+      const int b = e % rb, g = e / rb;  // neighbouring threads: neighbouring row blocks
+      const int gr = r0 + 8 * b, gk = k0 + 8 * g;
+      uint16_t v[8][8];  // v[j][i]: row gr + i, k gk + j
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const bool kin = gk + j < kmax;
+        if (vec && kin && gr + 8 <= rmax) {
+          const uint4 q = *reinterpret_cast<const uint4*>(X + gr + (long)(gk + j) * sk);
+          const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            v[j][2 * i] = (uint16_t)(w[i] & 0xFFFFu);
+            v[j][2 * i + 1] = (uint16_t)(w[i] >> 16);
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 8; i++)
+            v[j][i] = (kin && gr + i < rmax) ? bf_at(X, (long)(gr + i) * sr + (long)(gk + j) * sk)
+                                             : (uint16_t)0;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        uint4 q;
+        q.x = v[0][i] | ((uint32_t)v[1][i] << 16);
+        q.y = v[2][i] | ((uint32_t)v[3][i] << 16);
+        q.z = v[4][i] | ((uint32_t)v[5][i] << 16);
+        q.w = v[6][i] | ((uint32_t)v[7][i] << 16);
+        *reinterpret_cast<uint4*>(dst + ((size_t)g * R + 8 * b + i) * 8) = q;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    gemm_tc(const bf16* __restrict__ A, long sAm, long sAk, const bf16* __restrict__ B,
+            long sBk, long sBn, float* __restrict__ C, long ldc, int M, int N, int K, int nt,
+            int tcols, int accumulate, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint16_t* sa[2] = {reinterpret_cast<uint16_t*>(smem),
+                     reinterpret_cast<uint16_t*>(smem + kGtStageA + kGtStageB)};
+  uint16_t* sb[2] = {reinterpret_cast<uint16_t*>(smem + kGtStageA),
+                     reinterpret_cast<uint16_t*>(smem + 2 * kGtStageA + kGtStageB)};
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * (kGtStageA + kGtStageB));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int m0 = blockIdx.y * kTcRows, n0 = blockIdx.x * nt;
+  const uint32_t bar_a[2] = {smem_addr(bar), smem_addr(bar + 1)};
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a[0]) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a[1]) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(tmem_slot)),
+                 "r"(tcols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = instr_desc(nt);
+  const int chunks = (K + kGtKc - 1) / kGtKc;
+  bool ok = true;
+  int issued = 0;  // chunks whose MMAs were committed
+  for (int c = 0; c < chunks; c++) {
+    const int s = c & 1;
+    if (c >= 2) {  // the MMAs of chunk c - 2 read this stage
+      ok = mbar_wait(bar_a[s], (uint32_t)(((c - 2) >> 1) & 1));
+      ok = __syncthreads_and(ok) != 0;
+      if (!ok) break;
+    }
+    const int k0 = c * kGtKc;
+    const int kc = min(kGtKc, ((K - k0 + 15) / 16) * 16);  // a multiple of 16, zero past K
+    stage_operand(A, sAm, sAk, m0, M, k0, K, kTcRows, kc, sa[s], tid);
+    stage_operand(B, sBn, sBk, n0, N, k0, K, nt, kc, sb[s], tid);
+    // the generic-proxy stores become visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a0 = smem_addr(sa[s]), b0 = smem_addr(sb[s]);
+      for (int ks = 0; ks < kc / 16; ks++) {
+        const uint64_t ad = smem_desc(a0 + ks * 2 * (kTcRows * 16), kTcRows * 16, 128);
+        const uint64_t bd = smem_desc(b0 + ks * 2 * (nt * 16), nt * 16, 128);
+        const uint32_t accum = (c > 0 || ks > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(accum)
+            : "memory");
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              bar_a[s])
+          : "memory");
+    }
+    issued = c + 1;
+  }
+  // the last commit covers every MMA this thread issued before it; the other stage's
+  // last commit has then arrived as well
+  if (ok && issued > 0) {
+    const int c = issued - 1;
+    ok = mbar_wait(bar_a[c & 1], (uint32_t)((c >> 1) & 1));
+    if (ok && c >= 1) ok = mbar_wait(bar_a[(c - 1) & 1], (uint32_t)(((c - 1) >> 1) & 1));
+    ok = __syncthreads_and(ok) != 0;
+  }
+  tc_fence_after();
+  if (ok && issued > 0) {
+    const int r = m0 + warp * 32 + (tid & 31);
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    const bool vec_c = (reinterpret_cast<uintptr_t>(C) & 15u) == 0 && (ldc % 4) == 0;
+#pragma unroll 1
+    for (int c0 = 0; c0 < nt; c0 += 16) {
+      uint32_t v[16];
+      tmem_ld16(lane_base + (uint32_t)c0, v);
+      if (r < M) {
+        float* o = C + (long)r * ldc + n0 + c0;
+        if (vec_c && n0 + c0 + 16 <= N) {  // four 16-byte stores along the row
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            float4 w = make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                   __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
+            float4* p4 = reinterpret_cast<float4*>(o) + j;
+            if (accumulate) {
+              const float4 c = *p4;
+              w.x += c.x;
+              w.y += c.y;
+              w.z += c.z;
+              w.w += c.w;
+            }
+            *p4 = w;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            if (n0 + c0 + j < N)
+              o[j] = accumulate ? o[j] + __uint_as_float(v[j]) : __uint_as_float(v[j]);
+          }
+        }
+      }
+    }
+  } else if (issued > 0) {
+    // a wait gave up: wait once more (bounded) for the MMAs in flight before the tensor
+    // memory is released, and report it
+    const int c = issued - 1;
+    mbar_wait(bar_a[c & 1], (uint32_t)((c >> 1) & 1));
+    if (c >= 1) mbar_wait(bar_a[(c - 1) & 1], (uint32_t)(((c - 1) >> 1) & 1));
+    if (tid == 0) atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(tcols)
+                 : "memory");
+}
+
 // W[K x N] (FP32, row-major) -> BF16 W^T[N x K] in the operand layout of mlp_infer_tc
 __global__ void to_bf16_operand(const float* __restrict__ Wf, int K, int N, bf16* __restrict__ out) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -623,10 +782,21 @@ int cast_weights(mcs_surrogate* s, cudaStream_t st) {
   return MCS_OK;
 }
 
-void gemm(cudaStream_t st, const bf16* A, long sAm, long sAk, const bf16* B, long sBk, long sBn,
-          float* C, long ldc, int M, int N, int K, bool accumulate) {
-  const dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
-  gemm_bf16<<<grid, 128, 0, st>>>(A, sAm, sAk, B, sBk, sBn, C, ldc, M, N, K, accumulate ? 1 : 0);
+// The tile width: the widest of 256 ... 16 columns (an MMA's N) that still gives the grid
+// 256 CTAs (two per SM fit in shared and tensor memory), so that the staging loads of
+// many CTAs are in flight at once and the small weight-gradient GEMMs (M = 32 or 256 over
+// K = the batch) spread over the SMs.
+void gemm(cudaStream_t st, int* err, const bf16* A, long sAm, long sAk, const bf16* B,
+          long sBk, long sBn, float* C, long ldc, int M, int N, int K, bool accumulate) {
+  int nt = std::min(kTcCols, ((N + 15) / 16) * 16);
+  const int mt = (M + kTcRows - 1) / kTcRows;
+  while (nt > 16 && (long)mt * ((N + nt - 1) / nt) < 256) nt /= 2;
+  nt = std::max(16, (nt / 16) * 16);
+  int tcols = 32;
+  while (tcols < nt) tcols <<= 1;
+  const dim3 grid((unsigned)((N + nt - 1) / nt), (unsigned)mt);
+  gemm_tc<<<grid, kTcThreads, kGtSmem, st>>>(A, sAm, sAk, B, sBk, sBn, C, ldc, M, N, K, nt,
+                                             tcols, accumulate ? 1 : 0, err);
 }
 
 // forward of rows already in A.xb; final FP32 output in A.z[3]
@@ -634,7 +804,7 @@ void forward(mcs_surrogate* s, Acts& A, int rows, cudaStream_t st) {
   const bf16* x = A.xb;
   for (int l = 0; l < kLayers; l++) {
     const int K = kK[l], N = kN[l];
-    gemm(st, x, K, 1, s->Wb[l], N, 1, A.C, N, rows, N, K, false);
+    gemm(st, s->err, x, K, 1, s->Wb[l], N, 1, A.C, N, rows, N, K, false);
     const long n = (long)rows * N;
     const bool last = l == kLayers - 1;
     bias_act<<<blocks(n, 256), 256, 0, st>>>(A.C, s->params + kLay.b[l], rows, N, A.z[l],
@@ -649,11 +819,11 @@ void backward(mcs_surrogate* s, Acts& A, int rows, cudaStream_t st) {
     const int K = kK[l], N = kN[l];
     const bf16* ain = l == 0 ? A.xb : A.a[l - 1];
     // dW = a_in^T dz ; db = colsum(dz)
-    gemm(st, ain, 1, K, A.dzb, N, 1, s->grad + kLay.W[l], N, K, N, rows, false);
+    gemm(st, s->err, ain, 1, K, A.dzb, N, 1, s->grad + kLay.W[l], N, K, N, rows, false);
     col_sum<<<N, 256, 0, st>>>(A.dz, rows, N, s->grad + kLay.b[l]);
     if (l > 0) {
       // dh = dz W^T ; dz_prev = dh * silu'(z_prev)
-      gemm(st, A.dzb, N, 1, s->Wb[l], 1, N, A.dh, K, rows, K, N, false);
+      gemm(st, s->err, A.dzb, N, 1, s->Wb[l], 1, N, A.dh, K, rows, K, N, false);
       const long n = (long)rows * K;
       silu_back<<<blocks(n, 256), 256, 0, st>>>(A.dh, A.z[l - 1], n, A.dz, A.dzb);
     }
@@ -676,6 +846,8 @@ void loss_grad(mcs_surrogate* s, Acts& A, int rows, cudaStream_t st) {
 int surrogate_reserve(mcs_surrogate* s) {
   MCS_CUDA_RET(cudaFuncSetAttribute(mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     kTcSmem));
+  MCS_CUDA_RET(cudaFuncSetAttribute(gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kGtSmem));
   return MCS_OK;
 }
 
@@ -706,7 +878,7 @@ int surrogate_check(mcs_surrogate* s) {
   MCS_CUDA_RET(cudaMemcpy(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost));
   if (e) {
     cudaMemset(s->err, 0, sizeof(int));
-    return fail(MCS_ERR_CUDA, "surrogate inference: a tensor-core wait timed out");
+    return fail(MCS_ERR_CUDA, "surrogate: a tensor-core wait timed out");
   }
   return MCS_OK;
 }
@@ -865,6 +1037,8 @@ int mcs_surrogate_grad(mcs_surrogate* s, const float* X, const float* y, size_t 
   cudaFree(dX);
   cudaFree(dy);
   if (e != cudaSuccess) return fail(MCS_ERR_CUDA, "gradient failed: %s", cudaGetErrorString(e));
+  rc = surrogate_check(s);
+  if (rc) return rc;
   *loss = ls / (float)n;
   return MCS_OK;
 }
@@ -1000,6 +1174,7 @@ int mcs_surrogate_train(mcs_surrogate* s, const float* X, const float* y, size_t
   }
   cudaStreamSynchronize(st);
   cleanup();
+  if (!rc) rc = surrogate_check(s);  // a training GEMM whose tensor-core wait timed out
   if (!rc) s->trained = true;
   return rc;
 }

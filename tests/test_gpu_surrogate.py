@@ -46,7 +46,7 @@ def test_forward_matches_fp64_reference(ctx, params, feats):
 def test_tensor_core_inference_many_tiles(ctx, params, feats):
     """Inference runs on the tcgen05 kernel (128-row tiles, persistent CTAs).  39963 rows
     need several tiles per CTA and end in a ragged tile; the outputs match the FP64
-    reference MLP and give the same NLL as the training forward (mma.sync kernels)."""
+    reference MLP and give the same NLL as the training forward (the GEMM kernel)."""
     import mlp_ref as R
     from mcs import Surrogate
 
