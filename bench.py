@@ -337,6 +337,8 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool, repeats: 
         return times, plan.results()
 
     g_spec = default_guide_opts()
+    g_skip = default_guide_opts()
+    g_skip.skip_top = 1e-3  # skip the a_max trial where the model gives it < 0.1 %
     g_br = default_guide_opts()
     g_br.mode = A.GUIDE_BRACKET
     sv.opts.max_buckets, tuned = T.autotune(ctx, sv.setups, sv.modals, sv.points, sv.opts,
@@ -347,7 +349,8 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool, repeats: 
         plain_t, plain = run(pp)
         pp.close()
         for name, model, g in (("speculate", sur, g_spec), ("bracket", sur, g_br),
-                               ("speculate_untrained", untrained, g_spec)):
+                               ("speculate_untrained", untrained, g_spec),
+                               ("speculate_skip_top", sur, g_skip)):
             gp = ctx.plan(sv.setups, sv.modals, sv.points, sv.opts, surrogate=model, guide=g)
             t, r = run(gp)
             arms[name] = (t, r, gp.guide_info())
@@ -406,6 +409,10 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool, repeats: 
         "max_rel_err_vs_plain": main["max_rel_err_vs_plain"],
         "trained_vs_untrained_prior": main["value"] / st["speculate_untrained"]["value"],
         "untrained_prior": st["speculate_untrained"],
+        "skip_top_1e-3": dict(st["speculate_skip_top"],
+                              note="the a_max trial skipped where the predicted probability "
+                                   "of a stable a_max is below 0.1 %; not exact where that "
+                                   "prediction is wrong"),
         "bracket": st["bracket"],
         "fp64_subset": len(sub),
         "within_2pct_of_gpu_fp64": main["within_2pct_of_gpu_fp64"],
@@ -427,6 +434,8 @@ def guided_serve(ctx, torch, stream, flush, device: int, no_cpu: bool, repeats: 
         r64, _ = O.solve_batch(setups, modals, P, sv.opts, nthreads=cpu_cores())
         res["within_2pct_of_cpu_fp64"] = within(arms["speculate"][1][sub], r64)
         res["bracket"]["within_2pct_of_cpu_fp64"] = within(arms["bracket"][1][sub], r64)
+        res["skip_top_1e-3"]["within_2pct_of_cpu_fp64"] = within(
+            arms["speculate_skip_top"][1][sub], r64)
         res["plain_within_2pct_of_cpu_fp64"] = within(plain[sub], r64)
     return res
 

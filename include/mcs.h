@@ -370,7 +370,11 @@ typedef struct {
   int32_t refine;      /* bisection iterations inside a verified bracket (3) */
   int32_t mode;        /* MCS_GUIDE_SPECULATE (default) or MCS_GUIDE_BRACKET */
   int32_t levels;      /* speculate: bisection levels, >= 1; above opts->iters: iters (8) */
-  int32_t pad;
+  float skip_top;      /* speculate: a point whose predicted probability of being stable at
+                          a_max is below this skips the plain first trial at a_max (0, the
+                          default: never).  Such a point is not reported open, so where the
+                          prediction is wrong and a_max is stable its limit differs from the
+                          plain one; every other point keeps the plain bracket. */
 } mcs_guide_opts;
 
 /* How each point of a guided solve was decided. */

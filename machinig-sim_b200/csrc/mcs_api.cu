@@ -618,6 +618,7 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
     ga.refine = pl->gopts.refine;
     ga.mode = pl->gopts.mode;
     ga.levels = pl->gopts.levels;
+    ga.skip_top = pl->gopts.skip_top;
   }
   const bool forked = !captured && nb > 1;
   if (forked) MCS_CUDA(cudaEventRecord(ctx->fork, s0));
@@ -710,7 +711,8 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
   if (sur && (!g || !(g->z > 0) || !(g->hw_min > 0) || !(g->hw_max >= g->hw_min) ||
               !(g->hw_direct > 0) || g->refine < 0 || g->refine > 30 ||
               (g->mode != MCS_GUIDE_SPECULATE && g->mode != MCS_GUIDE_BRACKET) ||
-              (g->mode == MCS_GUIDE_SPECULATE && g->levels < 1)))
+              (g->mode == MCS_GUIDE_SPECULATE && g->levels < 1) ||
+              !(g->skip_top >= 0.f && g->skip_top <= 1.f)))
     return fail(MCS_ERR_ARG, "guide options out of range");
   std::vector<PointParams> pp(n_points);
   std::vector<int> smem(n_points), slots(n_points), modes(n_points), nls(n_points),

@@ -114,6 +114,7 @@ struct GuideArgs {
   int refine = 0;                 // halvings of a hw_min bracket
   int mode = 0;                   // MCS_GUIDE_SPECULATE or MCS_GUIDE_BRACKET
   int levels = 0;                 // speculate: bisection levels
+  float skip_top = 0.f;           // speculate: P(stable at a_max) below this skips that trial
 };
 
 // One chatterAt trial of the batch kernel.

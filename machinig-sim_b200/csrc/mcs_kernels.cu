@@ -845,6 +845,21 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         return nit;
       };
       auto refine = [&]() { bisect(glo, ghi, refine_iters()); };
+      // the speculating guide: the plain bisection for `levels` levels, its rounds steered
+      // by N(mu, sigma) of the log depth
+      auto speculate_from = [&]() {
+        const double sg = g.sigma != nullptr ? (double)g.sigma[pi] : 1.0;
+        prior.normal = true;
+        prior.mu = (double)g.guide[pi].x;
+        prior.inv_sigma = 1.0 / fmax(sg, 1e-3);
+        bisect(o.a_min, o.a_max, min(g.levels, o.iters));
+      };
+      // a point predicted stable at a_max with a probability below skip_top starts at the
+      // bisection (its first trial at a_max is skipped)
+      if (speculate && g.skip_top > 0.f && g.sigma != nullptr) {
+        const double z = ((double)g.guide[pi].x - log(o.a_max)) / fmax((double)g.sigma[pi], 1e-3);
+        if (normcdf(z) < (double)g.skip_top) speculate_from();
+      }
       while (state != kDone) {
         // ---- plan the round ----
         Groups G;
@@ -927,12 +942,7 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
           } else if (!guided) {
             bisect(o.a_min, o.a_max, o.iters);
           } else if (speculate) {
-            // the plain bisection for `levels` levels, its rounds steered by N(mu, sigma)
-            const double sg = g.sigma != nullptr ? (double)g.sigma[pi] : 1.0;
-            prior.normal = true;
-            prior.mu = (double)g.guide[pi].x;
-            prior.inv_sigma = 1.0 / fmax(sg, 1e-3);
-            bisect(o.a_min, o.a_max, min(g.levels, o.iters));
+            speculate_from();
           } else {
             const float2 gd = g.guide[pi];
             const double hw = (double)gd.y;

@@ -913,7 +913,7 @@ void mcs_default_guide_opts(mcs_guide_opts* o) {
   o->refine = 3;
   o->mode = MCS_GUIDE_SPECULATE;
   o->levels = 8;
-  o->pad = 0;
+  o->skip_top = 0.f;
 }
 
 int mcs_surrogate_create(mcs_ctx* ctx, uint64_t seed, mcs_surrogate** out) {

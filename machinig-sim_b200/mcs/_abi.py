@@ -367,7 +367,7 @@ class TrainOpts(C.Structure):
 class GuideOpts(C.Structure):
     _fields_ = [("z", C.c_float), ("hw_min", C.c_float), ("hw_max", C.c_float),
                 ("hw_direct", C.c_float), ("refine", C.c_int32), ("mode", C.c_int32),
-                ("levels", C.c_int32), ("pad", C.c_int32)]
+                ("levels", C.c_int32), ("skip_top", C.c_float)]
 
 
 GUIDE_SPECULATE = 0

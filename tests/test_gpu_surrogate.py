@@ -252,6 +252,18 @@ def test_speculative_guide_is_the_plain_bisection(ctx, trained_small):
     g.levels = 99
     again, _ = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts, g)
     assert again.tobytes() == plain.tobytes()
+    # skip_top = 1: every point skips the first trial at a_max; the points that chatter
+    # there keep their bracket and spend one trial and one round less, the open ones are
+    # no longer reported open
+    g.levels = 8
+    g.skip_top = 1.0
+    sk, skinfo = ctx.solve_guided(s, wl.setups, wl.modals, wl.points, wl.opts, g)
+    assert np.all(sk["open"] == 0)
+    for f in ("alim", "lo", "hi"):
+        assert np.array_equal(sk[f][~op], res[f][~op]), f
+    assert np.all(sk["trials"][~op] == res["trials"][~op] - 1)
+    assert np.array_equal(skinfo["rounds"][~op], info["rounds"][~op] - 1)
+    g.skip_top = 0.0
     # serial trials: one trial per round, the same results
     o = wl.opts.__class__.from_buffer_copy(wl.opts)
     o.serial_trials = 1
