@@ -293,7 +293,11 @@ class Context:
 
     def solve_guided(self, surrogate, setups, modals, points, opts: A.Opts,
                      guide: A.GuideOpts | None = None):
-        """(results, guide info) of the surrogate-guided solve."""
+        """(results, guide info) of the surrogate-guided solve.
+
+        guide.mode GUIDE_SPECULATE (the default) runs the plain bisection's own trials for
+        guide.levels levels, steered by the prediction (the bracket is the plain one after
+        those levels); GUIDE_BRACKET verifies and refines a predicted bracket."""
         b = Batch(setups, modals, points)
         n = len(b.points)
         out = np.zeros(max(1, n), dtype=A.RESULT_DTYPE)
