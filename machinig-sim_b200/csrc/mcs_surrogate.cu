@@ -788,6 +788,7 @@ int cast_weights(mcs_surrogate* s, cudaStream_t st) {
 // K = the batch) spread over the SMs.
 void gemm(cudaStream_t st, int* err, const bf16* A, long sAm, long sAk, const bf16* B,
           long sBk, long sBn, float* C, long ldc, int M, int N, int K, bool accumulate) {
+  if (M <= 0 || N <= 0 || K <= 0) return;  // nothing to multiply (never an empty grid)
   int nt = std::min(kTcCols, ((N + 15) / 16) * 16);
   const int mt = (M + kTcRows - 1) / kTcRows;
   while (nt > 16 && (long)mt * ((N + nt - 1) / nt) < 256) nt /= 2;
