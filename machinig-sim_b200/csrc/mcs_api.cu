@@ -362,6 +362,7 @@ struct mcs_plan {
   // surrogate guidance (guided plans)
   mcs_surrogate* sur = nullptr;
   mcs_guide_opts gopts{};
+  double a_max = 0.0;  // the bisection's upper end (the guide's skip_top test)
   DevBuf feat, gmu, gsigma, guide, ginfo;
   std::vector<Bucket> buckets;
   DevBuf params, order, results, queues, items;
@@ -492,6 +493,7 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
   order.clear();
   order.reserve(n_all);
   if (n_all == 0) return MCS_OK;
+  bool any_head = false;  // a multi-warp head leads the batch
   // resident blocks per SM and grid of a bucket, which then joins the list
   auto place = [&](Bucket& b) -> int {
     int bps = 0;
@@ -502,6 +504,23 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
                   cudaGetErrorString((cudaError_t)rc));
     if (bps < 1)
       return fail(MCS_ERR_UNSUPPORTED, "a %d-byte warp does not fit on an SM", b.smem);
+    // An FP64 linear bucket takes the kernel held to more resident warps when its shared
+    // memory lets them reside: a warp of it runs at 0.87 of the default's speed (spilled
+    // words), and the SM's rate grows with its resident warps (measured on one B200:
+    // 148 x k uniform points, k = 1 ... 8 warps per SM in proportion), so it pays from
+    // 10 resident warps against the default's 8.  Only in a batch bound by its total work:
+    // beside a multi-warp head (a batch bound by its slowest points) the extra resident
+    // warps slowed the head (768-speed sweep: 119 -> 136 ms).
+    if (!trials && !any_head && b.shape.fp64 && !b.shape.nl && !b.shape.grouped &&
+        b.shape.coop == 0) {
+      KernelShape dk = b.shape;
+      dk.dense = 1;
+      int dbps = 0;
+      if (occupancy_solve(dk, b.smem, &dbps) == 0 && 0.87 * dbps > (double)bps) {
+        b.shape = dk;
+        bps = dbps;
+      }
+    }
     b.blocks_per_sm = bps;
     b.grid = (int)std::min<long long>(b.count, (long long)bps * ctx->sms);
     buckets.push_back(b);
@@ -509,7 +528,8 @@ int make_buckets(mcs_ctx* ctx, const std::vector<int>& smem, const std::vector<d
   };
   int rc = MCS_OK;
   std::vector<char> in_head(n_all, 0);
-  if (!trials && pp && coop_warps > 1 && coop_head > 0) {
+  any_head = !trials && pp && coop_warps > 1 && coop_head > 0;
+  if (any_head) {
     std::vector<int32_t> members;
     std::vector<Bucket> heads;
     coop_head_buckets(cost, slots, modes, nls, grps, *pp, fp64, coop_warps, coop_head,
@@ -581,7 +601,8 @@ int enqueue_guide(mcs_plan* pl, cudaStream_t s0) {
   return surrogate_predict_device(pl->sur, static_cast<const float*>(pl->feat.p), (long)pl->n,
                                   static_cast<float*>(pl->gmu.p),
                                   static_cast<float*>(pl->gsigma.p),
-                                  static_cast<float2*>(pl->guide.p), &pl->gopts, s0);
+                                  static_cast<float2*>(pl->guide.p), &pl->gopts, s0,
+                                  pl->a_max);
 }
 
 // Enqueue the plan's work: zero the queue counters, (optionally) the surrogate's
@@ -618,7 +639,6 @@ int enqueue(mcs_plan* pl, cudaStream_t s0, const mcs_opts* o, const volatile int
     ga.refine = pl->gopts.refine;
     ga.mode = pl->gopts.mode;
     ga.levels = pl->gopts.levels;
-    ga.skip_top = pl->gopts.skip_top;
   }
   const bool forked = !captured && nb > 1;
   if (forked) MCS_CUDA(cudaEventRecord(ctx->fork, s0));
@@ -796,6 +816,7 @@ int build_plan(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs
     pl->sur = sur;
     surrogate_hold(sur, +1);
     pl->gopts = *g;
+    pl->a_max = o->a_max;
     std::vector<float> f(n_points * MCS_FEATURES);
     for (size_t i = 0; i < n_points; i++)
       point_features(setups[points[i].setup], modals[points[i].modal], points[i].S, *o,

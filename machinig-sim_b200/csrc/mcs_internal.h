@@ -114,7 +114,6 @@ struct GuideArgs {
   int refine = 0;                 // halvings of a hw_min bracket
   int mode = 0;                   // MCS_GUIDE_SPECULATE or MCS_GUIDE_BRACKET
   int levels = 0;                 // speculate: bisection levels
-  float skip_top = 0.f;           // speculate: P(stable at a_max) below this skips that trial
 };
 
 // One chatterAt trial of the batch kernel.
@@ -132,6 +131,7 @@ struct KernelShape {
   int nl;     // 1: size effect and/or process damping present
   int grouped = 0;  // 1: points may run several trials per warp in lane groups
   int coop = 0;     // > 0: solve with this many warps per point (multi-warp bisection)
+  int dense = 0;    // 1: the FP64 linear solve held to more resident warps per SM
 };
 
 // Host launchers (mcs_kernels.cu).  chained = 1: a programmatic dependent launch behind the
@@ -189,7 +189,7 @@ inline int set_smem_limits() {
 // surrogate (mcs_surrogate.cu)
 int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d_mu,
                              float* d_sigma, float2* d_guide, const mcs_guide_opts* g,
-                             cudaStream_t st);
+                             cudaStream_t st, double a_max);
 int surrogate_reserve(mcs_surrogate* s);
 // after a synchronise: MCS_ERR_CUDA if an inference kernel timed out waiting for its MMAs
 int surrogate_check(mcs_surrogate* s);

@@ -756,8 +756,13 @@ __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane
 }
 
 // Persistent solve: each warp takes points from the queue and runs timeDomainLimit.
-template <typename T, int SLOTS, int NM, bool NL, bool GR>
-__global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const PointParams* __restrict__ pts,
+// MINW: resident warps per SM the register allocation is held to.  The default leaves it
+// to the compiler; kDenseWarps is the variant the host picks for FP64 linear buckets whose
+// shared memory lets more warps reside than the default's registers do (a few spilled
+// words, a slower warp, more of them: see the host's bucket placement).
+constexpr int kDenseWarps = 12;
+template <typename T, int SLOTS, int NM, bool NL, bool GR, int MINW = MinWarps<T>::value>
+__global__ void __launch_bounds__(kWarp, MINW) solve_kernel(const PointParams* __restrict__ pts,
                                                       const int32_t* __restrict__ order, int n,
                                                       DevOpts o, mcs_result* __restrict__ out,
                                                       unsigned int* __restrict__ queue,
@@ -854,12 +859,9 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) solve_kernel(const 
         prior.inv_sigma = 1.0 / fmax(sg, 1e-3);
         bisect(o.a_min, o.a_max, min(g.levels, o.iters));
       };
-      // a point predicted stable at a_max with a probability below skip_top starts at the
-      // bisection (its first trial at a_max is skipped)
-      if (speculate && g.skip_top > 0.f && g.sigma != nullptr) {
-        const double z = ((double)g.guide[pi].x - log(o.a_max)) / fmax((double)g.sigma[pi], 1e-3);
-        if (normcdf(z) < (double)g.skip_top) speculate_from();
-      }
+      // a point the inference marked (predicted stable at a_max with a probability below
+      // skip_top) starts at the bisection: its first trial at a_max is skipped
+      if (speculate && g.guide[pi].y < -1.5f) speculate_from();
       while (state != kDone) {
         // ---- plan the round ----
         Groups G;
@@ -1207,7 +1209,12 @@ __global__ void __launch_bounds__(kWarp, MinWarps<T>::value) trials_kernel(const
 }
 
 template <typename T, int SLOTS, int NM>
-void* solve_fn(bool nl, bool gr) {
+void* solve_fn(bool nl, bool gr, bool dense) {
+#if MCS_PREC == 64
+  if (dense && !nl && !gr)
+    return reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, false, false, kDenseWarps>);
+#endif
+  if (dense) return nullptr;
   if (gr)
     return nl ? reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, true, true>)
               : reinterpret_cast<void*>(&solve_kernel<T, SLOTS, NM, false, true>);
@@ -1232,7 +1239,7 @@ void* pick(bool solve, const KernelShape& s) {
   if (s.slots == SL && s.modes == NMV)                                                 \
     return !solve ? trials_fn<KScalar, SL, NMV>(s.nl)                                  \
                   : s.coop > 0 ? coop_fn<KScalar, SL, NMV>(s.nl)                       \
-                               : solve_fn<KScalar, SL, NMV>(s.nl, s.grouped);
+                               : solve_fn<KScalar, SL, NMV>(s.nl, s.grouped, s.dense);
   MCS_PICK(1, 1)
   MCS_PICK(1, 2)
   MCS_PICK(1, 3)
@@ -1252,10 +1259,15 @@ int set_smem_limits() {
   for (int nl = 0; nl < 2; nl++)
   for (int sl = 1; sl <= kMaxSlots; sl++)
     for (int nm = 1; nm <= kMaxModes; nm++)
-      for (int k = 0; k < 4; k++) {  // solve, grouped solve, trials, multi-warp solve
+      for (int k = 0; k < 5; k++) {  // solve, grouped solve, trials, multi-warp, dense solve
         KernelShape ks{sl, nm, fp, nl, k == 1 ? 1 : 0};
         if (k == 3) ks.coop = kCoopMaxWarps;
+        if (k == 4) {
+          if (!fp || nl) continue;  // the dense variant: FP64 linear solves only
+          ks.dense = 1;
+        }
         void* f = pick(k != 2, ks);
+        if (!f) return (int)cudaErrorInvalidValue;
         cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              k == 3 ? kCoopSmemLimit : kMaxSmemPerWarp);
         if (e != cudaSuccess) return (int)e;

@@ -253,7 +253,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     mlp_infer_tc(const float* __restrict__ X, long n, const float* __restrict__ params,
                  TcWeights tw, float* __restrict__ mu, float* __restrict__ sigma,
                  float2* __restrict__ guide, float z, float hw_min, float hw_max,
-                 float hw_direct, int* __restrict__ err) {
+                 float hw_direct, int spec, float skip_top, float log_amax,
+                 int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   bf16* A = reinterpret_cast<bf16*>(smem);
   bf16* W = reinterpret_cast<bf16*>(smem + kTcSmemA);
@@ -379,7 +380,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           if (sigma) sigma[row] = sv;
           if (guide) {
             const float w = z * sv;
-            guide[row] = make_float2(m, w > hw_direct ? -1.f : fminf(fmaxf(w, hw_min), hw_max));
+            float gy = w > hw_direct ? -1.f : fminf(fmaxf(w, hw_min), hw_max);
+            // the speculating guide: -2 marks a point that skips its first trial at a_max
+            // (predicted stable there with a probability below skip_top)
+            if (spec) gy = (skip_top > 0.f && normcdff((m - log_amax) / sv) < skip_top) ? -2.f : -1.f;
+            guide[row] = make_float2(m, gy);
           }
         }
       }
@@ -857,7 +862,7 @@ int surrogate_reserve(mcs_surrogate* s) {
 // bisection.
 int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d_mu,
                              float* d_sigma, float2* d_guide, const mcs_guide_opts* g,
-                             cudaStream_t st) {
+                             cudaStream_t st, double a_max) {
   if (n <= 0) return MCS_OK;
   int rc = surrogate_reserve(s);
   if (rc) return rc;
@@ -868,7 +873,9 @@ int surrogate_predict_device(mcs_surrogate* s, const float* dX, long n, float* d
   const int grid = (int)std::min<long>(tiles, std::max(1, s->sms));
   mlp_infer_tc<<<grid, kTcThreads, kTcSmem, st>>>(
       dX, n, s->params, tw, d_mu, d_sigma, d_guide, g ? g->z : 0.f, g ? g->hw_min : 0.f,
-      g ? g->hw_max : 0.f, g ? g->hw_direct : 0.f, s->err);
+      g ? g->hw_max : 0.f, g ? g->hw_direct : 0.f,
+      g && g->mode == MCS_GUIDE_SPECULATE ? 1 : 0, g ? g->skip_top : 0.f,
+      a_max > 0.0 ? (float)std::log(a_max) : 0.f, s->err);
   MCS_CUDA_RET(cudaGetLastError());
   return MCS_OK;
 }
@@ -1194,7 +1201,7 @@ int mcs_surrogate_predict(mcs_surrogate* s, const float* X, size_t n, float* mu,
   }
   cudaStream_t st = ctx_stream(s->ctx);
   cudaMemcpyAsync(dX, X, n * kIn * sizeof(float), cudaMemcpyHostToDevice, st);
-  rc = surrogate_predict_device(s, dX, (long)n, dmu, dsg, nullptr, nullptr, st);
+  rc = surrogate_predict_device(s, dX, (long)n, dmu, dsg, nullptr, nullptr, st, 0.0);
   cudaError_t e = cudaStreamSynchronize(st);
   if (!rc && e == cudaSuccess) rc = surrogate_check(s);
   if (!rc && e == cudaSuccess) e = cudaMemcpy(mu, dmu, n * sizeof(float), cudaMemcpyDeviceToHost);
