@@ -760,7 +760,9 @@ __device__ __forceinline__ bool read_cancel(const volatile int* cancel, int lane
 // to the compiler; kDenseWarps is the variant the host picks for FP64 linear buckets whose
 // shared memory lets more warps reside than the default's registers do (a few spilled
 // words, a slower warp, more of them: see the host's bucket placement).
+#if MCS_PREC == 64
 constexpr int kDenseWarps = 12;
+#endif
 template <typename T, int SLOTS, int NM, bool NL, bool GR, int MINW = MinWarps<T>::value>
 __global__ void __launch_bounds__(kWarp, MINW) solve_kernel(const PointParams* __restrict__ pts,
                                                       const int32_t* __restrict__ order, int n,
