@@ -330,8 +330,9 @@ int mcs_tune(mcs_ctx* ctx, const mcs_setup* setups, size_t n_setups, const mcs_m
  * The guided solve either speculates the plain bisection's next levels where the
  * prediction puts them, or verifies the bracket exp(mu -+ hw) with two time-domain
  * trials, refines it by bisection and falls back to the full bisection when a
- * verification fails (mcs_guide_opts.mode).  No counterpart in the reference: it accelerates timeDomainLimit (stabtd.js:24),
- * whose plain algorithm remains the judge of every result.
+ * verification fails (mcs_guide_opts.mode).  No counterpart in the reference: it
+ * accelerates timeDomainLimit (stabtd.js:24), whose plain algorithm every result is
+ * checked against.
  */
 #define MCS_FEATURES 20
 

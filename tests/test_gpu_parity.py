@@ -72,7 +72,7 @@ def ran_away(ref):
 
 
 def ill_conditioned(g, rows, ref, precision):
-    """FP64 is judged against the reference's response to a 1e-7 feed change, FP32 against
+    """FP64 is compared with the reference's response to a 1e-7 feed change, FP32 against
     changes up to 1e-5 (what an FP32 trajectory accumulates)."""
     levels = g["sens_levels"]
     use = levels <= (1e-5 if precision == "fp32" else 1e-7)
