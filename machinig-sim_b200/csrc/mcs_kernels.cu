@@ -823,11 +823,13 @@ __global__ void __launch_bounds__(kWarp, MINW) solve_kernel(const PointParams* _
       const bool guided = g.guide != nullptr && (speculate || g.guide[pi].y >= 0.f);
       const bool can_group = GR && P->groups > 1;
       int path = guided ? MCS_PATH_GUIDED : MCS_PATH_DIRECT;
-      // where the speculative rounds look: the bracket widths, or the prediction
+      // where the speculative rounds look: the prediction when there is one (either guide
+      // method, every bisection of the point: the plain fallback and the direct path too),
+      // else the bracket widths
       Prior prior;
-      prior.normal = false;
-      prior.mu = 0.0;
-      prior.inv_sigma = 0.0;
+      prior.normal = g.guide != nullptr && g.sigma != nullptr;
+      prior.mu = prior.normal ? (double)g.guide[pi].x : 0.0;
+      prior.inv_sigma = prior.normal ? 1.0 / fmax((double)g.sigma[pi], 1e-3) : 0.0;
       SpecPlan sp;
       sp.n = 0;
       int state = kTop, it = 0, iters = o.iters, nrounds = 0;
@@ -854,13 +856,7 @@ __global__ void __launch_bounds__(kWarp, MINW) solve_kernel(const PointParams* _
       auto refine = [&]() { bisect(glo, ghi, refine_iters()); };
       // the speculating guide: the plain bisection for `levels` levels, its rounds steered
       // by N(mu, sigma) of the log depth
-      auto speculate_from = [&]() {
-        const double sg = g.sigma != nullptr ? (double)g.sigma[pi] : 1.0;
-        prior.normal = true;
-        prior.mu = (double)g.guide[pi].x;
-        prior.inv_sigma = 1.0 / fmax(sg, 1e-3);
-        bisect(o.a_min, o.a_max, min(g.levels, o.iters));
-      };
+      auto speculate_from = [&]() { bisect(o.a_min, o.a_max, min(g.levels, o.iters)); };
       // a point the inference marked (predicted stable at a_max with a probability below
       // skip_top) starts at the bisection: its first trial at a_max is skipped
       if (speculate && g.guide[pi].y < -1.5f) speculate_from();
