@@ -16,7 +16,7 @@ HEADER = ROOT / "include" / "mcs.h"
 
 STRUCTS = ["mcs_mode", "mcs_modal", "mcs_tool", "mcs_material", "mcs_setup", "mcs_point",
            "mcs_opts", "mcs_result", "mcs_trial", "mcs_trial_result", "mcs_lobe_query",
-           "mcs_plan_info"]
+           "mcs_plan_info", "mcs_train_opts", "mcs_guide_opts", "mcs_guide_info"]
 
 
 def declared_functions() -> list[str]:
@@ -34,7 +34,10 @@ def c_sizes(tmp_path_factory):
               "mcs_setup": ["tool", "mat", "arc_st", "fz"],
               "mcs_modal": ["nx", "x", "y"],
               "mcs_lobe_query": ["Ktc", "rpm_max", "modal"],
-              "mcs_plan_info": ["n_points", "h2d_bytes", "d2h_bytes"]}
+              "mcs_plan_info": ["n_points", "h2d_bytes", "d2h_bytes"],
+              "mcs_train_opts": ["lr", "seed", "keep_best"],
+              "mcs_guide_opts": ["z", "refine", "mode", "levels", "skip_top"],
+              "mcs_guide_info": ["mu", "sigma", "path", "rounds"]}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(){"]
     for s in STRUCTS:
         lines.append(f'printf("{s} %zu\\n", sizeof({s}));')
@@ -56,7 +59,8 @@ def test_struct_layouts(c_sizes):
              "mcs_material": A.Material, "mcs_setup": A.Setup, "mcs_point": A.Point,
              "mcs_opts": A.Opts, "mcs_result": A.Result, "mcs_trial": A.Trial,
              "mcs_trial_result": A.TrialResult, "mcs_lobe_query": A.LobeQuery,
-             "mcs_plan_info": A.PlanInfo}
+             "mcs_plan_info": A.PlanInfo, "mcs_train_opts": A.TrainOpts,
+             "mcs_guide_opts": A.GuideOpts, "mcs_guide_info": A.GuideInfo}
     for name, ct in pairs.items():
         assert c_sizes[name] == C.sizeof(ct), name
     dtypes = {"mcs_modal": A.MODAL_DTYPE, "mcs_setup": A.SETUP_DTYPE, "mcs_point": A.POINT_DTYPE,
