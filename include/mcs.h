@@ -30,7 +30,8 @@
 extern "C" {
 #endif
 
-#define MCS_ABI_VERSION 1
+#define MCS_ABI_VERSION 2 /* 2: mcs_guide_opts gained mode, levels and skip_top;
+                             mcs_guide_info reports rounds */
 #define MCS_MAX_MODES 4 /* modes per axis (frf.js fitModes keeps at most 4) */
 #define MCS_MAX_TEETH 8
 #define MCS_BINS 180    /* angular bins of the engagement map, cutting.js:15 */
