@@ -517,6 +517,250 @@ def worker_latency(ctx, torch, precision: str, repeats: int = 3) -> dict:
     return out
 
 
+# The Simulator's defaults (sim.js:44-50): D 10 mm, 3 flutes, helix 30, flute 25 mm, stickout
+# 30 mm on a 50 kN/mm spindle, 5 um runout, modal zeta 0.04; A5052 (materials.js:25); a frame
+# spends dynBudget = 220,000 slice-force evaluations (sim.js:50, "about 5 ms of JS").
+SIM_TOOL = {"D": 10.0, "N": 3, "helixDeg": 30.0, "type": "flat", "fluteLen": 25.0,
+            "stickout": 30.0, "kSpindle": 50000.0, "runout": 5.0}
+A5052 = {"Ktc": 700.0, "Krc": 210.0, "Kac": 120.0, "Kte": 20.0, "Kre": 25.0, "Kae": 5.0,
+         "mc": 0.10, "Ci": 2e4}
+DYN_BUDGET = 220000
+
+
+def _pool_map(fn, items, threads: int):
+    """fn over items on `threads` host threads (the oracle's ctypes calls release the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        return list(ex.map(fn, items))
+
+
+def _event_ms(torch, stream, call) -> float:
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    call()
+    b.record(stream)
+    b.synchronize()
+    return float(a.elapsed_time(b))
+
+
+def playback_leg(ctx, torch, stream, no_cpu: bool, repeats: int = 5,
+                 n: int = 148 * 8) -> dict:
+    """The playback dynamics (CuttingEngine.run as Simulator.step drives it, sim.js:396-416):
+    engines of the Simulator's default tool in a half-immersion down-milling cut with the
+    thin wall engaged, each frame one dynBudget of slice-force evaluations.  `value` is a
+    batch of 1184 engines (8 per SM) at spread speeds running frame after frame; `frame_ms`
+    is one engine's frame, the interactive case.  The host restatement runs a sample of the
+    same engines on every host thread, and its statistics check the GPU's."""
+    import math
+
+    from mcs import engine as E
+    from mcs import spindle as SP
+
+    tm = SP.tool_model(SIM_TOOL)
+    modal = {"k": tm["k"], "fn": tm["fn"], "zeta": 0.04}
+    tool = {k: SIM_TOOL[k] for k in ("N", "helixDeg", "type", "fluteLen", "runout")}
+    tool["R"] = SIM_TOOL["D"] / 2
+    ap, fz = 2.0, 0.05
+    wall = {"k": 800.0, "m": 0.05, "zeta": 0.02, "nx": 0.0, "ny": 1.0}
+    nz = math.ceil(ap / max(0.25, SIM_TOOL["fluteLen"] / 48))  # slices (cutting.js:63,103)
+    cost = SIM_TOOL["N"] * nz                                   # sim.js:409
+    steps = DYN_BUDGET // cost
+    speeds = np.linspace(8000.0, 16000.0, n)
+    cfgs = [E.config(tool, modal, A5052, s) for s in speeds]
+    g = E.engagement(E.arc_map(math.pi / 2, math.pi), (1, 0), fz, -ap, ap, wall=wall)
+    out = {"workload": f"{n} engines 8000-16000 rpm, Simulator default tool (D10, 3 flutes, "
+                       f"stickout 30, 5 um runout), A5052, half-immersion down milling, "
+                       f"ap {ap} mm ({nz} slices), fz {fz}, thin wall; a frame = "
+                       f"{steps} steps = {steps * cost} slice-force evaluations (dynBudget)",
+           "unit": "slice-force evaluations/s", "precision": "fp64"}
+    eng = E.Engines(ctx, n)
+    try:
+        eng.configure(cfgs)
+        eng.set_engagement([g] * n)
+        arr = np.full(n, steps, dtype=np.int64)
+        eng.run(arr)  # warm-up frame
+        ts = [_event_ms(torch, stream, lambda: eng.run(arr)) for _ in range(repeats)]
+        st = eng.take_stats()
+    finally:
+        eng.close()
+    ms = float(np.median(ts))
+    out["value"] = n * steps * cost / (ms / 1e3)
+    out["batch_frame_ms"] = ms
+    out["gpu_launches_per_frame"] = 1
+    one = E.Engines(ctx, 1)
+    try:
+        one.configure([cfgs[n // 2]])
+        one.set_engagement([g])
+        a1 = np.array([steps], dtype=np.int64)
+        one.run(a1)
+        t1 = [_event_ms(torch, stream, lambda: one.run(a1)) for _ in range(repeats)]
+        w1 = []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            one.run(a1)
+            w1.append(1e3 * (time.perf_counter() - t0))
+    finally:
+        one.close()
+    out["frame_ms"] = float(np.median(t1))
+    out["frame_e2e_ms"] = float(np.median(w1))
+    out["reference_frame_budget_ms"] = 5.0  # sim.js:50
+    if no_cpu:
+        return out
+    import pyoracle as O
+
+    cores = cpu_cores()
+    sample = list(range(0, n, max(1, n // (4 * cores))))
+
+    def host(i):
+        e = O.Engine()
+        e.configure_from(cfgs[i])
+        e.engage(g)
+        t = time.perf_counter()
+        for _ in range(1 + repeats):
+            e.run(steps)
+        dt = time.perf_counter() - t
+        return dt, e.take_stats_full()
+
+    t = time.perf_counter()
+    res = _pool_map(host, sample, cores)
+    wall_s = time.perf_counter() - t
+    evals = len(sample) * (1 + repeats) * steps * cost
+    one_thread = float(np.median([r[0] for r in res])) / (1 + repeats)
+    out["cpu_baseline"] = {"value": evals / wall_s, "unit": out["unit"], "cores": cores,
+                           "kind": "port",
+                           "sample": f"{len(sample)} of the engines, {1 + repeats} frames each, "
+                                     "C++ FP64 restatement of cutting.js, all host threads",
+                           "frame_ms_one_thread": 1e3 * one_thread}
+    rel, steps_equal = 0.0, True
+    for i, (_, ref) in zip(sample, res):
+        for f in ("sumFx", "sumFy", "sumT", "sumF"):
+            rel = max(rel, abs(float(st[i][f]) / float(ref[f]) - 1))
+        steps_equal &= int(st[i]["n"]) == int(ref["n"])
+    out["parity"] = {"engines_checked": len(sample), "max_rel_diff_force_sums": rel,
+                     "step_counts_equal": bool(steps_equal)}
+    out["vs_cpu"] = out["value"] / out["cpu_baseline"]["value"]
+    return out
+
+
+def composite_leg(ctx, no_cpu: bool, repeats: int = 5) -> dict:
+    """The chart's speed-dependent lobe diagram (Simulator.lobes, sim.js:262-287): a
+    diagram per 1000 rpm with the spindle model's modes at the node, read every 25 rpm,
+    for the Simulator's default tool; one call of mcs.compositeLobes against the host
+    restatement of the same loop, and the samples compared."""
+    import math
+
+    import mcs
+    from mcs import spindle as SP
+
+    sp = SP.Spindle.from_tool({k: SIM_TOOL[k] for k in ("D", "stickout", "kSpindle")},
+                              {"auto": True, "k": 0, "fn": 0, "zeta": 0.04})
+    base = {"N": 3, "Ktc": A5052["Ktc"], "Krc": A5052["Krc"], "phiSt": math.pi / 2,
+            "phiEx": math.pi, "lobes": 30, "rpmMin": 2000, "rpmMax": 40000}
+    got = mcs.compositeLobes(sp, base, ctx=ctx)[0]  # warm-up
+    ts = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        got = mcs.compositeLobes(sp, base, ctx=ctx)[0]
+        ts.append(1e3 * (time.perf_counter() - t0))
+    out = {"workload": f"Simulator default tool, 3 flutes, A5052, half immersion, 30 lobes, "
+                       f"2000-40000 rpm: {len(got)} samples",
+           "unit": "ms per diagram (e2e through mcs.compositeLobes)", "lower_is_better": True,
+           "value": float(np.median(ts))}
+    if no_cpu:
+        return out
+    import pyoracle as O
+
+    t0 = time.perf_counter()
+    ref = O.composite_lobes(sp.record, base, sp.frfs)[0]
+    out["cpu_baseline"] = {"value": 1e3 * (time.perf_counter() - t0), "unit": "ms per diagram",
+                           "cores": 1, "kind": "port",
+                           "sample": "the same diagram, restatement of sim.js:262-287 and "
+                                     "sld.js (Python node loop, C++ lobes), one thread"}
+    g = np.array([p["alim"] for p in got])
+    r = np.array([p["alim"] for p in ref])
+    out["parity"] = {"samples": len(g), "max_rel_diff": float(np.max(np.abs(g / r - 1)))}
+    out["vs_cpu"] = out["cpu_baseline"]["value"] / out["value"]
+    return out
+
+
+def identify_leg(ctx, no_cpu: bool, repeats: int = 5) -> dict:
+    """The identification's unit-force runs (identify.js:26-40): per cutting test six
+    rigid-tool engines, one per coefficient, two revolutions dropped and one averaged;
+    256 seeded tests (1536 engines) in one mcs.identify.unit_forces call against the host
+    restatement on every host thread, and the forces compared."""
+    from mcs import engine as E
+    from mcs import identify as I
+
+    tool = {k: SIM_TOOL[k] for k in ("D", "N", "helixDeg", "fluteLen")}
+    rng = np.random.default_rng(5)
+    tests = [{"fz": float(rng.uniform(0.02, 0.1)), "ap": float(rng.uniform(0.5, 5.0)),
+              "ae": float(rng.uniform(1.0, 10.0)), "mode": ("slot", "down", "up")[i % 3]}
+             for i in range(256)]
+    U = I.unit_forces(ctx, tool, tests)  # warm-up
+    ts = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        U = I.unit_forces(ctx, tool, tests)
+        ts.append(1e3 * (time.perf_counter() - t0))
+    ms = float(np.median(ts))
+    out = {"workload": f"{len(tests)} seeded tests (slot/down/up, fz 0.02-0.1, ap 0.5-5, "
+                       f"ae 1-10) of a D10 3-flute tool, 6 unit-force engines each",
+           "unit": "tests/s (e2e through mcs.identify.unit_forces)", "value": len(tests) / ms * 1e3,
+           "ms_per_call": ms}
+    if no_cpu:
+        return out
+    import pyoracle as O
+
+    cfgs, gs = [], []
+    for t in tests:
+        st, ex = I.immersion(t["mode"], t["ae"], tool["D"])
+        for key in I.COEF_KEYS:
+            mat = dict.fromkeys(I.COEF_KEYS, 0.0)
+            mat.update({key: 1.0, "mc": 0.0, "Ci": 0.0})
+            tl = I._engine_tool(tool, t["ap"], phase=0.0)
+            tl["nonlinear"] = False
+            cfgs.append(E.config(tl, E.RIGID, mat, 6000))
+            gs.append(E.engagement(E.arc_map(st, ex), (1, 0), t["fz"], -t["ap"], t["ap"]))
+    cores = cpu_cores()
+    chunks = [list(range(k, len(tests), cores)) for k in range(cores)]
+
+    def host(ch):
+        sel = [6 * j + c for j in ch for c in range(6)]
+        return ch, O.unit_forces_ref([cfgs[s] for s in sel], [gs[s] for s in sel])
+
+    t0 = time.perf_counter()
+    res = _pool_map(host, chunks, cores)
+    dt = time.perf_counter() - t0
+    ref = np.zeros_like(U)
+    for ch, r in res:
+        ref[ch] = r.reshape(len(ch), 6, 3)
+    scale = np.maximum(np.abs(ref).max(axis=2, keepdims=True), 1e-300)
+    out["cpu_baseline"] = {"value": len(tests) / dt, "unit": "tests/s", "cores": cores,
+                           "kind": "port",
+                           "sample": "the same tests, C++ FP64 restatement of identify.js "
+                                     "unitForces, all host threads"}
+    out["parity"] = {"tests": len(tests),
+                     "max_rel_diff": float(np.max(np.abs(U - ref) / scale))}
+    out["vs_cpu"] = out["value"] / out["cpu_baseline"]["value"]
+    return out
+
+
+def rows_leg(ctx, torch, stream, no_cpu: bool) -> dict:
+    """The rows around the stability path, each beside its host restatement.  A leg that
+    raises is recorded with its error; the headline line is printed regardless."""
+    legs = {"playback": lambda: playback_leg(ctx, torch, stream, no_cpu),
+            "composite_lobes": lambda: composite_leg(ctx, no_cpu),
+            "identify": lambda: identify_leg(ctx, no_cpu)}
+    out = {}
+    for name, leg in legs.items():
+        try:
+            out[name] = leg()
+        except Exception as e:  # noqa: BLE001  (recorded in the line, not swallowed)
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
+
+
 def make_workload(name: str, rank: int, points: int = 0):
     from mcs import workloads as W
 
@@ -764,6 +1008,8 @@ def ours(args) -> int:
                   if world == 1 and not args.no_guided else None)
         latency = (worker_latency(ctx, torch, args.precision)
                    if world == 1 and not args.no_latency else None)
+        rows = (rows_leg(ctx, torch, stream, args.no_cpu)
+                if world == 1 and not args.no_rows else None)
         line = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
@@ -789,6 +1035,7 @@ def ours(args) -> int:
                              if small else {})} or None,
             "guided": guided,
             "worker_latency": latency,
+            "rows": rows,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -819,6 +1066,8 @@ def main(argv=None) -> int:
     ap.add_argument("--guided-repeats", type=int, default=5)
     ap.add_argument("--no-latency", action="store_true",
                     help="skip the latency of the Worker's 18-speed request")
+    ap.add_argument("--no-rows", action="store_true",
+                    help="skip the playback engines, composite lobes and identification legs")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "hetero", "small"],
                     help="sweep (the headline), the heterogeneous batch or the 64-speed case")
     ap.add_argument("--max-buckets", type=int, default=0,
