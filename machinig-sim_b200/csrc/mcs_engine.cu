@@ -122,96 +122,99 @@ __global__ void __launch_bounds__(32) engine_run_kernel(const EngCfg* __restrict
   double sHb = 0, sB = 0, sRb = 0;  // this lane's share of sumHb, sumB, sumRb
   int ts_i = S.ts_i, h_i = S.h_i;
   long long ts_count = S.ts_count, h_count = S.h_count;
-  // this lane's slices (two slots) and end ring
-  const int k0 = lane, k1 = lane + 32;
+  // a step's evaluations, tooth-major (e = i * nz + k for the flutes, i * kR + j for the end
+  // rings), are spread over the lanes: lane l takes e = l, l + 32, ...; every tooth's
+  // evaluations run side by side instead of one tooth after another
+  const int ne = N * nz, nend = G.fza != 0 ? N * kR : 0;
   for (long long s = 0; s < n_steps; s++) {
     const double theta = pr * dphi;
     const double rx = x - w * wnx, ry = y - w * wny;
     const double xm = rx * 1e3, ym = ry * 1e3;
     double Fx = 0, Fy = 0, Fz = 0, T = 0, Fr2z = 0, Fsum = 0;
     const double rvx = vxs - wv * wnx, rvy = vys - wv * wny;
-    for (int i = 0; i < N; i++) {
-      bool engaged = false;
+    unsigned teeth = 0;  // bit i: tooth i engaged on this lane
+    for (int e = lane; e < ne; e += 32) {
+      const int i = e / nz, k = e - i * nz;
       const double dRi = C.dR[i];
       int pi = pr + i * spt;
       if (pi >= spr) pi -= spr;
-      for (int slot = 0; slot < 2; slot++) {
-        const int k = slot ? k1 : k0;
-        if (k >= nz) continue;
-        double phi = angle_mod(theta + i * pitch - G.sliceLag[k]);
-        if (phi < 0) phi += kTwoPi;
+      double phi = angle_mod(theta + i * pitch - G.sliceLag[k]);
+      if (phi < 0) phi += kTwoPi;
+      double sn, cs;
+      sincos(phi, &sn, &cs);
+      const double nxg = sn * ux + cs * vx, nyg = sn * uy + cs * vy;
+      const double rn = xm * nxg + ym * nyg + dRi;
+      float* cell = surf + (size_t)k * spr + pi;
+      const double prev = *cell;
+      const double feedH = fz * sn * G.sliceKap[k];
+      // Hb[(phi * binScale) | 0]: a bin past the map reads undefined, and undefined <= z
+      // is false
+      const double bs = phi * binScale;
+      const int bin = bs == bs ? (int)bs : 0;
+      const bool hbOut = bin < MCS_BINS && (double)G.Hb[bin] <= G.sliceZ[k];
+      if (hbOut || sn <= 0) {
+        *cell = (float)rn;
+        continue;
+      }
+      double h = feedH + rn - prev;
+      if (h <= 0) {  // tooth out of cut: the old surface survives one more feed step
+        *cell = (float)(prev - feedH);
+        continue;
+      }
+      *cell = (float)rn;
+      if (h > hMax) h = hMax;
+      const double se = mc != 0 ? pow(kHRef / (h > kHMin ? h : kHMin), mc) : 1.0;
+      const double bk = G.sliceB[k];
+      const double Ft = Ktc * se * h * bk + Kte * bk;
+      double Fr = Krc * se * h * bk + Kre * bk;
+      const double Fa = Kac * se * h * bk + Kae * bk;
+      if (pdK != 0) Fr += pdK * (bk / G.db) / G.sliceR[k] * (rvx * nxg + rvy * nyg);
+      const double txg = cs * ux - sn * vx, tyg = cs * uy - sn * vy;
+      Fx += -Ft * txg - Fr * nxg;
+      Fy += -Ft * tyg - Fr * nyg;
+      Fz -= Fa;
+      T += Ft * G.sliceR[k];
+      const double fr = hypot(Ft, Fr);
+      Fsum += fr;
+      Fr2z += fr * (G.sliceZ[k] - G.tipZ);
+      teeth |= 1u << i;
+      sHb += h * bk;
+      sB += bk;
+      sRb += G.sliceR[k] * h * bk;
+    }
+    for (int e = lane; e < nend; e += 32) {
+      // end edges at the tip (no helix lag): thrust, torque and in-plane tangential force
+      const int i = e / kR, j = e - i * kR;
+      double phi = angle_mod(theta + i * pitch);
+      if (phi < 0) phi += kTwoPi;
+      const int row = ((int)(phi / kTwoPi * kE)) * kR;
+      // an angle of exactly 2 pi would read past the map (undefined in the reference)
+      const double depth = row < kE * kR ? (double)G.Eb[row + j] : 0.0;
+      if (depth > 2e-4) {
         double sn, cs;
         sincos(phi, &sn, &cs);
-        const double nxg = sn * ux + cs * vx, nyg = sn * uy + cs * vy;
-        const double rn = xm * nxg + ym * nyg + dRi;
-        float* cell = surf + (size_t)k * spr + pi;
-        const double prev = *cell;
-        const double feedH = fz * sn * G.sliceKap[k];
-        // Hb[(phi * binScale) | 0]: a bin past the map reads undefined, and undefined <= z
-        // is false
-        const double bs = phi * binScale;
-        const int bin = bs == bs ? (int)bs : 0;
-        const bool hbOut = bin < MCS_BINS && (double)G.Hb[bin] <= G.sliceZ[k];
-        if (hbOut || sn <= 0) {
-          *cell = (float)rn;
-          continue;
-        }
-        double h = feedH + rn - prev;
-        if (h <= 0) {  // tooth out of cut: the old surface survives one more feed step
-          *cell = (float)(prev - feedH);
-          continue;
-        }
-        *cell = (float)rn;
-        if (h > hMax) h = hMax;
-        const double se = mc != 0 ? pow(kHRef / (h > kHMin ? h : kHMin), mc) : 1.0;
-        const double bk = G.sliceB[k];
-        const double Ft = Ktc * se * h * bk + Kte * bk;
-        double Fr = Krc * se * h * bk + Kre * bk;
-        const double Fa = Kac * se * h * bk + Kae * bk;
-        if (pdK != 0) Fr += pdK * (bk / G.db) / G.sliceR[k] * (rvx * nxg + rvy * nyg);
         const double txg = cs * ux - sn * vx, tyg = cs * uy - sn * vy;
-        Fx += -Ft * txg - Fr * nxg;
-        Fy += -Ft * tyg - Fr * nyg;
-        Fz -= Fa;
-        T += Ft * G.sliceR[k];
-        const double fr = hypot(Ft, Fr);
-        Fsum += fr;
-        Fr2z += fr * (G.sliceZ[k] - G.tipZ);
-        engaged = true;
-        sHb += h * bk;
-        sB += bk;
-        sRb += G.sliceR[k] * h * bk;
+        const double c = G.ringCos[j], ds = G.ringDs[j];
+        const double h = (depth < G.fza ? depth : G.fza) * c;
+        const double se = mc != 0 ? pow(kHRef / (h > kHMin ? h : kHMin), mc) : 1.0;
+        const double Ft = Ktc * se * h * ds + Kte * ds;
+        const double Fn = Krc * se * h * ds + Kre * ds;
+        Fx += -Ft * txg;
+        Fy += -Ft * tyg;
+        Fz -= Fn * c;
+        T += Ft * G.ringR[j];
+        Fsum += Ft;
+        Fr2z += Ft * G.ringZ[j];
+        teeth |= 1u << i;
+        sHb += h * ds;
+        sB += ds;
+        sRb += G.ringR[j] * h * ds;
       }
-      if (G.fza != 0 && lane < kR) {
-        // end edges at the tip (no helix lag): thrust, torque and in-plane tangential force
-        double phi = angle_mod(theta + i * pitch);
-        if (phi < 0) phi += kTwoPi;
-        const int row = ((int)(phi / kTwoPi * kE)) * kR;
-        // an angle of exactly 2 pi would read past the map (undefined in the reference)
-        const double depth = row < kE * kR ? (double)G.Eb[row + lane] : 0.0;
-        if (depth > 2e-4) {
-          double sn, cs;
-          sincos(phi, &sn, &cs);
-          const double txg = cs * ux - sn * vx, tyg = cs * uy - sn * vy;
-          const double c = G.ringCos[lane], ds = G.ringDs[lane];
-          const double h = (depth < G.fza ? depth : G.fza) * c;
-          const double se = mc != 0 ? pow(kHRef / (h > kHMin ? h : kHMin), mc) : 1.0;
-          const double Ft = Ktc * se * h * ds + Kte * ds;
-          const double Fn = Krc * se * h * ds + Kre * ds;
-          Fx += -Ft * txg;
-          Fy += -Ft * tyg;
-          Fz -= Fn * c;
-          T += Ft * G.ringR[lane];
-          Fsum += Ft;
-          Fr2z += Ft * G.ringZ[lane];
-          engaged = true;
-          sHb += h * ds;
-          sB += ds;
-          sRb += G.ringR[lane] * h * ds;
-        }
-      }
-      if (__any_sync(kAll, engaged)) st.engTeeth += 1;
     }
+    // the ring cell tooth i reads was written one tooth period earlier by the lane of tooth
+    // i + 1: the warp barrier orders those global stores before the later loads
+    __syncwarp();
+    st.engTeeth += __popc(__reduce_or_sync(kAll, teeth));
     Fx = wsum(Fx);
     Fy = wsum(Fy);
     Fz = wsum(Fz);
@@ -223,17 +226,24 @@ __global__ void __launch_bounds__(32) engine_run_kernel(const EngCfg* __restrict
     y = 0;
     vxs = 0;
     vys = 0;
-    for (int j = 0; j < nmx; j++) {
-      v[0][j] += (Fx - C.mcd[0][j] * v[0][j] - C.mk[0][j] * q[0][j]) / C.mm[0][j] * dt;
-      q[0][j] += v[0][j] * dt;
-      x += q[0][j];
-      vxs += v[0][j];
+    // unrolled to the mode limit so that the modal states stay in registers
+#pragma unroll
+    for (int j = 0; j < MCS_MAX_MODES; j++) {
+      if (j < nmx) {
+        v[0][j] += (Fx - C.mcd[0][j] * v[0][j] - C.mk[0][j] * q[0][j]) / C.mm[0][j] * dt;
+        q[0][j] += v[0][j] * dt;
+        x += q[0][j];
+        vxs += v[0][j];
+      }
     }
-    for (int j = 0; j < nmy; j++) {
-      v[1][j] += (Fy - C.mcd[1][j] * v[1][j] - C.mk[1][j] * q[1][j]) / C.mm[1][j] * dt;
-      q[1][j] += v[1][j] * dt;
-      y += q[1][j];
-      vys += v[1][j];
+#pragma unroll
+    for (int j = 0; j < MCS_MAX_MODES; j++) {
+      if (j < nmy) {
+        v[1][j] += (Fy - C.mcd[1][j] * v[1][j] - C.mk[1][j] * q[1][j]) / C.mm[1][j] * dt;
+        q[1][j] += v[1][j] * dt;
+        y += q[1][j];
+        vys += v[1][j];
+      }
     }
     if (wk != 0) {  // the reaction on the wall along its normal (:250-258)
       const double Fw = -(Fx * wnx + Fy * wny);
