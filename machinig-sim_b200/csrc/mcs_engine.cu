@@ -4,11 +4,11 @@
 // The host derives everything configure() and setEngagement() compute (FP64, the
 // reference's expressions) and uploads it; the run kernel executes the run() loop
 // (cutting.js:146-296) with every term a cut has:
-//   * the flutes (:171-212): lane l owns slices l and l + 32 of every tooth, in the
-//     reference's tooth order; each evaluation takes the angle, the engagement-map bin,
-//     the regenerative chip, the size effect, process damping, the axial force and the
-//     torque, in FP64 with the surface ring in float;
-//   * the end edges (:213-237): lane j < 6 owns end ring j of every tooth;
+//   * the flutes (:171-212): a step's (tooth, slice) evaluations are spread over the
+//     lanes, all teeth side by side; each evaluation takes the angle, the engagement-map
+//     bin, the regenerative chip, the size effect, process damping, the axial force and
+//     the torque, in FP64 with the surface ring in float;
+//   * the end edges (:213-237): the (tooth, end ring) evaluations spread the same way;
 //   * the per-step sums (forces, torque, force-weighted height) by warp butterflies, the
 //     modal integration (:239-249) and the thin wall (:250-258) on every lane;
 //   * once-per-tooth samples, statistics and the decimated history (:259-292) by lane 0.
