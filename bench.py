@@ -20,6 +20,9 @@ A step = the whole 4096-point sweep.
 `workloads.hetero`  the heterogeneous batch (16384 seeded setups, process damping and size
          effect on, autotuned schedule, captured graph), measured the same way.
 `guided`  surrogate-guided serving of 65536 queries against the plain plan, repeated.
+`rows`   the playback engines (a batch of CuttingEngines, one dynBudget frame each), the
+         chart's composite lobe diagram and the identification's unit-force runs, each
+         beside the host restatement of the same runs and checked against it.
 Multi-GPU (torchrun): every rank solves its own seeded sweep (weak scaling, no collective
 on the data path); the time is the max over ranks.
 
