@@ -157,7 +157,7 @@ def node_probe() -> dict:
                                "deno, bun) on PATH")
     else:
         rec["reference_js"] = ("unavailable on this box: a runtime exists but the reference's "
-                               "JavaScript sources are not on the GPU box")
+                               "JavaScript sources are not on this machine")
     return rec
 
 
