@@ -44,6 +44,14 @@ def config(tool: Mapping[str, Any], modal: Mapping[str, Any], mat: Mapping[str, 
     return c
 
 
+def _fill_f32(dst, values) -> None:
+    """Copy values, as float32 and flattened, into the ctypes float array dst (same length)."""
+    a = np.ascontiguousarray(np.asarray(values, dtype=np.float32).ravel())
+    if a.size != len(dst):
+        raise ValueError(f"{a.size} values for {len(dst)} entries")
+    C.memmove(C.addressof(dst), a.ctypes.data, a.nbytes)
+
+
 def engagement(Hb, u=(1.0, 0.0), fz: float = 0.0, tipZ: float = 0.0, ap: float = 0.0, *,
                rAt: Callable[[float], float] | None = None, dz: float | None = None,
                Eb=None, fza: float = 0.0, rOut: float = 0.0,
@@ -55,7 +63,7 @@ def engagement(Hb, u=(1.0, 0.0), fz: float = 0.0, tipZ: float = 0.0, ap: float =
     (fza, rOut, zAt) with the end-face map Eb[36 * 6], setWork(wall {k, m, zeta, nx, ny})
     and setWear({Kte, Kre})."""
     g = A.Engagement()
-    g.Hb[:] = [float(v) for v in np.asarray(Hb, dtype=np.float32)]
+    _fill_f32(g.Hb, Hb)
     g.ux, g.uy = float(u[0]), float(u[1])
     g.fz, g.tip_z, g.ap = float(fz), float(tipZ), float(ap)
     if rAt is not None:
@@ -71,7 +79,7 @@ def engagement(Hb, u=(1.0, 0.0), fz: float = 0.0, tipZ: float = 0.0, ap: float =
             g.slice_kap[k] = 1 / math.sqrt(1 + dr * dr)
         g.profile = 1
     if Eb is not None:
-        g.Eb[:] = [float(v) for v in np.asarray(Eb, dtype=np.float32).ravel()]
+        _fill_f32(g.Eb, Eb)
     g.fza, g.end_r = float(fza), float(rOut)
     if fza > 0:
         za = zAt or (lambda r: 0.0)

@@ -64,13 +64,15 @@ def unit_forces(ctx, tool: Mapping[str, Any], tests: Sequence[Mapping[str, Any]]
     cfgs, gs = [], []
     for t in tests:
         st, ex = immersion(t["mode"], t["ae"], tool["D"])
+        # the test's six engines share one engagement (the record is copied per engine)
+        g = E.engagement(E.arc_map(st, ex), (1, 0), t["fz"], -t["ap"], t["ap"])
         for key in COEF_KEYS:
             mat = dict.fromkeys(COEF_KEYS, 0.0)
             mat.update({key: 1.0, "mc": mc, "Ci": 0.0})
             tl = _engine_tool(tool, t["ap"], phase=0.0)  # unitForces passes no phase
             tl["nonlinear"] = mc > 0
             cfgs.append(E.config(tl, E.RIGID, mat, 6000))
-            gs.append(E.engagement(E.arc_map(st, ex), (1, 0), t["fz"], -t["ap"], t["ap"]))
+            gs.append(g)
     if not cfgs:
         return np.zeros((0, 6, 3))
     eng = E.Engines(ctx, len(cfgs))
