@@ -69,3 +69,72 @@ def test_sync_average_fills_empty_bins_and_finds_a_ringing():
     coarse = np.arange(int(5 * 60 / S * 3000)) / 3000.0
     a = I.sync_average(coarse, [np.sin(2 * math.pi * S / 60 * coarse)] * 3, S)
     assert np.all(np.isfinite(a["avg"])) and np.any(a["cnt"] == 0) and a["avg"].shape == (3, 360)
+
+
+def test_engagement_records_and_unit_force_inputs():
+    """The engine records the host builds: a map of the wrong length is rejected, the map
+    and end-face arrays land in the record as float32 (infinities kept), and the unit-force
+    runs hand the library one configuration per coefficient with the test's engagement."""
+    import ctypes as C
+
+    import pytest
+
+    from mcs import _abi as A
+    from mcs import engine as E
+    from mcs import identify as I
+
+    with pytest.raises(ValueError):
+        E.engagement(np.zeros(A.BINS - 1), (1, 0), 0.05, -1.0, 1.0)
+    hb = np.where(np.arange(A.BINS) % 3 == 0, -np.inf, np.linspace(-1, 2, A.BINS))
+    eb = np.linspace(0, 0.3, A.END_BINS * A.END_RINGS).reshape(A.END_BINS, A.END_RINGS)
+    g = E.engagement(hb, (1, 0), 0.05, -1.0, 1.0, Eb=eb, fza=0.02, rOut=4.0)
+    assert np.array_equal(np.frombuffer(bytes(g.Hb), dtype=np.float32),
+                          hb.astype(np.float32))
+    assert np.array_equal(np.frombuffer(bytes(g.Eb), dtype=np.float32),
+                          eb.astype(np.float32).ravel())
+
+    seen = {}
+
+    class Recorder:  # stands in for the device engines
+        def __init__(self, ctx, n):
+            self.n = n
+
+        def configure(self, cfgs):
+            seen["cfg"] = [bytes(c) for c in cfgs]
+
+        def set_engagement(self, gs):
+            seen["eng"] = [bytes(x) for x in gs]
+
+        def run(self, steps):
+            seen.setdefault("steps", []).append(np.asarray(steps).copy())
+
+        def take_stats(self):
+            out = np.zeros(self.n, dtype=A.ENGINE_STATS_DTYPE)
+            out["n"] = 1
+            return out
+
+        def close(self):
+            pass
+
+    real = E.Engines
+    E.Engines = Recorder
+    try:
+        tool = {"D": 10.0, "N": 3, "helixDeg": 30.0, "fluteLen": 25.0}
+        tests = [{"fz": 0.05, "ap": 2.0, "ae": 10.0, "mode": "slot"},
+                 {"fz": 0.08, "ap": 1.0, "ae": 3.0, "mode": "down"}]
+        U = I.unit_forces(None, tool, tests)
+    finally:
+        E.Engines = real
+    assert U.shape == (2, 6, 3)
+    # one configuration per coefficient; both tests use the same tool (flute length
+    # max(25, ap + 1) = 25), so their six configurations agree
+    assert len(seen["cfg"]) == 12 and len(set(seen["cfg"][:6])) == 6
+    assert seen["cfg"][:6] == seen["cfg"][6:]
+    for t, test in enumerate(tests):
+        st, ex = I.immersion(test["mode"], test["ae"], tool["D"])
+        want = bytes(E.engagement(E.arc_map(st, ex), (1, 0), test["fz"], -test["ap"],
+                                  test["ap"]))
+        assert seen["eng"][6 * t: 6 * t + 6] == [want] * 6
+    # two revolutions, statistics dropped, one revolution
+    assert np.array_equal(seen["steps"][0], 2 * seen["steps"][1])
+    assert C.sizeof(A.Engagement) == len(seen["eng"][0])
